@@ -1,0 +1,354 @@
+"""Benchmark of the CSR hot path on B200.
+
+Default workload: plain CSR SpMV y = A x, float32 values, int32 column
+indices, on the 2,000,000 x 2,000,000 Zipf(2) matrix (row length
+min(50000, ceil(2.887 Z)), ~39M nonzeros, seed 1) -- the configuration the
+headline metric "CSR SpMV/SpMM GB/s vs HBM peak" is quoted on.  A step is one
+SpMV over the whole matrix.
+
+  value     algorithmic GB/s with A, x resident in HBM (CUDA events, L2
+            flushed between steps), summed over ranks / max rank time
+  e2e       the same metric through the public API with x copied from pinned
+            host memory and y read back every step
+  roofline  algorithmic bytes per launch / mean launch time vs measured HBM peak
+  cpu_baseline  the CPU oracle on the host cores, bounded sample
+
+``--impl reference`` times the CPU restatement of the reference's SpMV
+semantics (fp32 values, fp64 row sums) with all host threads.
+Multi-GPU (torchrun): each rank runs an independent replica (weak scaling);
+there is no data-path collective.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "CSR SpMV/SpMM GB/s vs HBM peak; bf16+autograd vs fp32 plain at stated error"
+
+
+# ---------------------------------------------------------------- helpers
+
+def _measured_peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _ncu_traffic(workload):
+    path = os.path.join(REPO, "profiles", "ncu_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    return d.get(workload)
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = str(gpu_index)
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", self.gpu],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- workloads
+
+class SpmvZipf:
+    name = "spmv_csr_zipf2_2Mx2M_f32"
+    dtype = "f32"
+
+    def __init__(self, device, seed=1):
+        import torch
+
+        import flagsparse_b200 as fs
+        from flagsparse_b200 import workloads
+
+        self.torch = torch
+        self.fs = fs
+        c = workloads.zipf_csr(n=2_000_000, seed=seed, dtype=np.float32)
+        self.host = c
+        self.M, self.K = c["shape"]
+        self.nnz = int(c["indices"].size)
+        self.device = device
+        self.data = torch.from_numpy(c["data"]).to(device)
+        self.indices = torch.from_numpy(c["indices"]).to(device)
+        self.indptr = torch.from_numpy(c["indptr"]).to(device)
+        self.x = torch.from_numpy(c["x"]).to(device)
+        self.prepared = fs.prepare_spmv_csr(self.data, self.indices, self.indptr, c["shape"])
+        self.y = torch.empty(self.M, dtype=torch.float32, device=device)
+        # pinned host buffers for the end-to-end leg
+        self.x_host = torch.from_numpy(c["x"]).pin_memory()
+        self.y_host = torch.empty(self.M, dtype=torch.float32).pin_memory()
+        self.x_dev2 = torch.empty_like(self.x)
+
+    def config(self):
+        return {"workload": self.name, "rows": self.M, "cols": self.K, "nnz": self.nnz,
+                "row_length": "min(50000, ceil(2.887*Z)), Z~Zipf(2) truncated at 50000",
+                "index_dtype": "int32", "indptr_dtype": "int64", "seed": 1,
+                "l2": "flushed between timed steps (256 MiB write)"}
+
+    def alg_bytes(self):
+        # values + column indices + row pointers + x once + y once
+        return self.nnz * (4 + 4) + (self.M + 1) * 8 + self.K * 4 + self.M * 4
+
+    def step(self):
+        self.fs.flagsparse_spmv_csr(x=self.x, prepared=self.prepared, out=self.y)
+
+    def e2e_step(self):
+        self.x_dev2.copy_(self.x_host, non_blocking=True)
+        self.fs.flagsparse_spmv_csr(x=self.x_dev2, prepared=self.prepared, out=self.y)
+        self.y_host.copy_(self.y, non_blocking=True)
+
+    def e2e_bytes(self):
+        return self.K * 4, self.M * 4
+
+    def cpu_run(self, nthreads):
+        from oracle import oracle
+
+        c = self.host
+        return oracle.spmv_f32_acc64(c["indptr"], c["indices"], c["data"], c["x"], nthreads=nthreads)
+
+
+def _cpu_measure(make_workload_host, budget_s, nthreads):
+    """Repeat the CPU oracle over the whole matrix until ~budget_s seconds; return (s per step, reps)."""
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        make_workload_host(nthreads)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or reps >= 200:
+            return el / reps, reps
+
+
+# ---------------------------------------------------------------- main
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="native", choices=["native", "reference"])
+    ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU-oracle work for cpu_baseline")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=device)
+
+    wl = SpmvZipf(device)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        wl.step()
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    for i in range(args.steps):
+        flush.fill_(float(i))
+        starts[i].record()
+        wl.step()
+        ends[i].record()
+    torch.cuda.synchronize()
+    barrier()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    t_ms = sum(step_ms)
+
+    # end-to-end through the public API with host buffers
+    for _ in range(2):
+        wl.e2e_step()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        wl.e2e_step()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    e2e_ms = e0.elapsed_time(e1)
+
+    if world > 1:
+        tt = torch.tensor([t_ms, e2e_ms], dtype=torch.float64, device=device)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms, e2e_ms = tt.tolist()
+
+    alg = wl.alg_bytes()
+    value = world * alg * args.steps / (t_ms * 1e-3) / 1e9
+    e2e_val = world * alg * args.steps / (e2e_ms * 1e-3) / 1e9
+    peak, peak_src = _measured_peaks()
+    mean_launch_ms = statistics.mean(step_ms)
+    achieved = alg / (mean_launch_ms * 1e-3) / 1e9
+    traffic = _ncu_traffic(wl.name)
+    h2d, d2h = wl.e2e_bytes()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import oracle
+
+        nthreads = oracle.max_threads()
+        s_per, reps = _cpu_measure(wl.cpu_run, args.cpu_budget, nthreads)
+        cpu = {"value": round(alg / s_per / 1e9, 3), "unit": "GB/s", "cores": nthreads, "kind": "port",
+               "sample": f"{reps} full SpMVs of the same matrix (fp32 values, fp64 row sums), "
+                         f"{s_per * 1e3:.1f} ms each, OpenMP over rows"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": round(value, 2),
+            "unit": "GB/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(t_ms / args.steps, 5),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": wl.dtype,
+            "data": "synthetic (seeded Zipf(2) power-law CSR, values/x U[-1,1])",
+            "config": dict(wl.config(), parallelism=f"replicas{world}" if world > 1 else "single"),
+            "e2e": {"value": round(e2e_val, 2), "unit": "GB/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs, copy burst)",
+                         "alg_bytes_per_launch": alg},
+            "cpu_baseline": cpu,
+            "gpu_launches": args.steps,
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args, rank, world):
+    """CPU restatement of the reference's SpMV semantics, all host threads, rank 0 only."""
+    if rank != 0:
+        return
+    from flagsparse_b200 import workloads
+    from oracle import oracle
+
+    c = workloads.zipf_csr(n=2_000_000, seed=1, dtype=np.float32)
+    nnz = int(c["indices"].size)
+    M, K = c["shape"]
+    alg = nnz * 8 + (M + 1) * 8 + K * 4 + M * 4
+    nthreads = oracle.max_threads()
+    for _ in range(args.warmup):
+        oracle.spmv_f32_acc64(c["indptr"], c["indices"], c["data"], c["x"], nthreads=nthreads)
+    # each step is one full SpMV; cap the number of steps so the run stays short
+    steps = args.steps
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        oracle.spmv_f32_acc64(c["indptr"], c["indices"], c["data"], c["x"], nthreads=nthreads)
+    el = time.perf_counter() - t0
+    value = alg * steps / el / 1e9
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": round(el / steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Zipf(2) power-law CSR, values/x U[-1,1])",
+        "config": {"workload": SpmvZipf.name, "rows": M, "cols": K, "nnz": nnz, "index_dtype": "int32",
+                   "parallelism": "host cores"},
+        "impl": "reference",
+        "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": nthreads, "kind": "port",
+                         "sample": f"{steps} full SpMVs, fp32 values with fp64 row sums (FlagSparse's fp32 "
+                                   "semantics), OpenMP over rows"},
+        "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

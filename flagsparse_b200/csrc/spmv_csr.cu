@@ -1,0 +1,465 @@
+// CSR SpMV y = A x for sm_100a.
+//
+// One launch covers the whole matrix.  Every warp executes one work unit of
+// the plan built by fsb_spmv_plan_build (plan.cu); a unit's 32-byte
+// descriptor carries its nonzero range, so the warp issues its value / column
+// loads immediately, and the dozens of resident warps per SM keep many
+// independent load chains in flight:
+//
+//  * row-block unit: a run of rows with < 2*cap <= 256 nonzeros.  Lanes load
+//    8 nonzeros each with coalesced evict-first loads (x keeps its L2 lines),
+//    gather x, park the products in the warp's shared-memory slice in
+//    compensated form, and teams of T lanes (T ~ mean row length, <= 32) sum
+//    the rows and reduce with shuffles.
+//  * long-row chunk: `chunk_nnz` nonzeros of one row with > cap nonzeros, in
+//    256-nonzero batches whose loads are issued one batch ahead.  A one-chunk
+//    row is written directly; otherwise the warp publishes a partial sum and
+//    the warp whose atomic ticket completes the row adds all partials in a
+//    fixed order and resets the ticket, so results are deterministic.
+//
+// Replaces _spmv_csr_real_kernel / _spmv_csr_complex_kernel
+// (sparse_operations/spmv_csr.py:179-240) and the bucketed CSR-vector kernels
+// (spmv_csr.py:247-368) of flagos-ai/FlagSparse.
+#include <type_traits>
+
+#include "fsb_common.cuh"
+
+namespace fsb {
+
+// Per-nonzero contribution, one (hi, lo) pair per real component when the
+// sum is compensated.  For the half types the fp32 product is exact, so lo
+// stays 0 and is not stored.
+template <int DT>
+struct SpmvTraits {
+  using V = VT<DT>;
+  using S = typename V::Store;
+  using R = typename V::Real;
+  static constexpr int kComp = V::kComplex ? 2 : 1;
+  static constexpr bool kLo = !V::kExactProduct;
+};
+
+template <typename S> __device__ __forceinline__ S to_store(float v);
+template <> __device__ __forceinline__ __half to_store<__half>(float v) { return __float2half_rn(v); }
+template <> __device__ __forceinline__ __nv_bfloat16 to_store<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
+template <> __device__ __forceinline__ float to_store<float>(float v) { return v; }
+template <typename S> __device__ __forceinline__ S to_store(double v) { return v; }
+
+// Row accumulator.  COMP = true: Dot2 compensated sums (Comp); COMP = false:
+// plain sums in the real type (Plain), used only where the caller opts in.
+template <int DT, bool COMP, bool CPLX = VT<DT>::kComplex>
+struct SpmvAcc;
+
+template <int DT, bool COMP>
+struct SpmvAcc<DT, COMP, false> {
+  using Tr = SpmvTraits<DT>;
+  using S = typename Tr::S;
+  using R = typename Tr::R;
+  static constexpr bool kLo = COMP && Tr::kLo;   // stored products carry their rounding error
+  static constexpr int kPartialReals = 2;
+  using Sum = typename std::conditional<COMP, Comp<R>, Plain<R>>::type;
+  Sum c;
+  __device__ __forceinline__ void zero() { c.zero(); }
+  // contribution of a*x; with kLo, hi + lo == a*x exactly
+  __device__ __forceinline__ static void prod(S a, S x, R* hi, R* lo) {
+    R ar = to_real(a), xr = to_real(x);
+    R p = mul_rn(ar, xr);
+    hi[0] = p;
+    if constexpr (kLo) lo[0] = fma_rn(ar, xr, -p);
+  }
+  __device__ __forceinline__ void add_prod(S a, S x) {
+    if constexpr (COMP) {
+      if constexpr (Tr::kLo) c.add_prod(to_real(a), to_real(x));
+      else c.add(mul_rn(to_real(a), to_real(x)));
+    } else {
+      c.add_prod(to_real(a), to_real(x));
+    }
+  }
+  __device__ __forceinline__ void add_rec(const R* hi, const R* lo) {
+    if constexpr (COMP) c.add_comp(hi[0], kLo ? lo[0] : R(0));
+    else c.add(hi[0]);
+  }
+  __device__ __forceinline__ void combine(const SpmvAcc& o) {
+    if constexpr (COMP) c.add_comp(o.c.hi, o.c.lo);
+    else c.add(o.c.hi);
+  }
+  __device__ __forceinline__ void shfl_combine(int m) {
+    SpmvAcc o = *this;
+    o.c.hi = __shfl_xor_sync(0xffffffffu, c.hi, m);
+    if constexpr (COMP) o.c.lo = __shfl_xor_sync(0xffffffffu, c.lo, m);
+    combine(o);
+  }
+  __device__ __forceinline__ void shfl_up(int o) {
+    c.hi = __shfl_up_sync(0xffffffffu, c.hi, o);
+    if constexpr (COMP) c.lo = __shfl_up_sync(0xffffffffu, c.lo, o);
+  }
+  __device__ __forceinline__ S result() const { return to_store<S>(c.value()); }
+  __device__ __forceinline__ void store(R* p) const {
+    p[0] = c.hi;
+    if constexpr (COMP) p[1] = c.lo;
+  }
+  __device__ __forceinline__ void load_cg(const R* p) {
+    c.hi = __ldcg(p);
+    if constexpr (COMP) c.lo = __ldcg(p + 1);
+  }
+};
+
+template <int DT, bool COMP>
+struct SpmvAcc<DT, COMP, true> {
+  using Tr = SpmvTraits<DT>;
+  using S = typename Tr::S;
+  using R = typename Tr::R;
+  static constexpr bool kLo = COMP;
+  static constexpr int kPartialReals = 4;
+  using Sum = typename std::conditional<COMP, Comp<R>, Plain<R>>::type;
+  Sum re, im;
+  __device__ __forceinline__ void zero() { re.zero(); im.zero(); }
+  // (ar + i ai)(xr + i xi): re = ar*xr - ai*xi, im = ar*xi + ai*xr.  With
+  // COMP each part is a compensated pair built from the exact products.
+  __device__ __forceinline__ static void prod(S a, S x, R* hi, R* lo) {
+    if constexpr (COMP) {
+      Comp<R> r, i;
+      r.zero(); i.zero();
+      r.add_prod(a.x, x.x); r.add_prod(-a.y, x.y);
+      i.add_prod(a.x, x.y); i.add_prod(a.y, x.x);
+      hi[0] = r.hi; lo[0] = r.lo; hi[1] = i.hi; lo[1] = i.lo;
+    } else {
+      hi[0] = fma_rn(a.x, x.x, -mul_rn(a.y, x.y));
+      hi[1] = fma_rn(a.x, x.y, mul_rn(a.y, x.x));
+    }
+  }
+  __device__ __forceinline__ void add_prod(S a, S x) {
+    re.add_prod(a.x, x.x); re.add_prod(-a.y, x.y);
+    im.add_prod(a.x, x.y); im.add_prod(a.y, x.x);
+  }
+  __device__ __forceinline__ void add_rec(const R* hi, const R* lo) {
+    if constexpr (COMP) { re.add_comp(hi[0], lo[0]); im.add_comp(hi[1], lo[1]); }
+    else { re.add(hi[0]); im.add(hi[1]); }
+  }
+  __device__ __forceinline__ void combine(const SpmvAcc& o) {
+    if constexpr (COMP) { re.add_comp(o.re.hi, o.re.lo); im.add_comp(o.im.hi, o.im.lo); }
+    else { re.add(o.re.hi); im.add(o.im.hi); }
+  }
+  __device__ __forceinline__ void shfl_combine(int m) {
+    SpmvAcc o = *this;
+    o.re.hi = __shfl_xor_sync(0xffffffffu, re.hi, m);
+    o.im.hi = __shfl_xor_sync(0xffffffffu, im.hi, m);
+    if constexpr (COMP) {
+      o.re.lo = __shfl_xor_sync(0xffffffffu, re.lo, m);
+      o.im.lo = __shfl_xor_sync(0xffffffffu, im.lo, m);
+    }
+    combine(o);
+  }
+  __device__ __forceinline__ void shfl_up(int o) {
+    re.hi = __shfl_up_sync(0xffffffffu, re.hi, o);
+    im.hi = __shfl_up_sync(0xffffffffu, im.hi, o);
+    if constexpr (COMP) {
+      re.lo = __shfl_up_sync(0xffffffffu, re.lo, o);
+      im.lo = __shfl_up_sync(0xffffffffu, im.lo, o);
+    }
+  }
+  __device__ __forceinline__ S result() const {
+    S s; s.x = re.value(); s.y = im.value(); return s;
+  }
+  __device__ __forceinline__ void store(R* p) const {
+    p[0] = re.hi; p[1] = re.lo; p[2] = im.hi; p[3] = im.lo;
+  }
+  __device__ __forceinline__ void load_cg(const R* p) {
+    re.hi = __ldcg(p); re.lo = __ldcg(p + 1); im.hi = __ldcg(p + 2); im.lo = __ldcg(p + 3);
+  }
+};
+
+template <typename T> __device__ __forceinline__ T ld_stream(const T* p) { return __ldcs(p); }
+template <> __device__ __forceinline__ __half ld_stream<__half>(const __half* p) {
+  unsigned short v = __ldcs(reinterpret_cast<const unsigned short*>(p));
+  return __ushort_as_half(v);
+}
+template <> __device__ __forceinline__ __nv_bfloat16 ld_stream<__nv_bfloat16>(const __nv_bfloat16* p) {
+  unsigned short v = __ldcs(reinterpret_cast<const unsigned short*>(p));
+  return __ushort_as_bfloat16(v);
+}
+template <typename T> __device__ __forceinline__ T ld_x(const T* p) { return __ldg(p); }
+
+constexpr int kSpmvWarps = 8;     // warps per block; one unit per warp
+constexpr int kSpmvItems = 8;     // nonzeros per lane per batch
+constexpr int kSpmvBatch = 32 * kSpmvItems;
+constexpr int kSpmvCap = kSpmvBatch / 2;  // row-block window: n < 2*cap <= batch
+
+struct UnitRegs { int64_t s0, s1; int32_t row, tag, nch; };
+
+__device__ __forceinline__ UnitRegs load_unit(const fsb_spmv_unit* u) {
+  const int4* p = reinterpret_cast<const int4*>(u);
+  int4 a = __ldg(p), b = __ldg(p + 1);
+  UnitRegs r;
+  r.s0 = (int64_t)(uint32_t)a.x | ((int64_t)a.y << 32);
+  r.s1 = (int64_t)(uint32_t)a.z | ((int64_t)a.w << 32);
+  r.row = b.x;
+  r.tag = b.y;
+  r.nch = b.z;
+  return r;
+}
+
+// Per-warp shared-memory slice, rounded to 16 bytes so every warp's slice
+// starts on a boundary that suits its widest element (double2 for c128).
+template <int DT, bool SHORT_COMP>
+static constexpr int spmv_warp_smem_bytes() {
+  using Tr = SpmvTraits<DT>;
+  constexpr bool lo = SpmvAcc<DT, SHORT_COMP>::kLo;
+  return (Tr::kComp * int(sizeof(typename Tr::R)) * (lo ? 2 : 1) * kSpmvBatch + 4 * (kSpmvCap + 1) + 15) & ~15;
+}
+
+// Resident blocks per SM the register budget is sized for: 8-byte reals and
+// complex values need more registers per thread than fp32 / half types.
+template <int DT>
+struct SpmvMinBlocks { static constexpr int value = (DT == FSB_C128) ? 2 : (DT == FSB_F64 || DT == FSB_C64) ? 3 : 4; };
+
+template <int DT, typename IT, typename PT, bool SHORT_COMP>
+__global__ void __launch_bounds__(kSpmvWarps * 32, SpmvMinBlocks<DT>::value)
+k_spmv_csr(const typename VT<DT>::Store* __restrict__ data, const IT* __restrict__ col,
+           const PT* __restrict__ ptr, const typename VT<DT>::Store* __restrict__ x,
+           typename VT<DT>::Store* __restrict__ y, fsb_spmv_plan plan) {
+  using Tr = SpmvTraits<DT>;
+  using S = typename Tr::S;
+  using R = typename Tr::R;
+  using Acc = SpmvAcc<DT, true>;  // long rows: always compensated
+  constexpr int NC = Tr::kComp;
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t unit = int64_t(blockIdx.x) * kSpmvWarps + warp;
+  if (unit >= plan.n_units) return;  // whole warp leaves together
+  const UnitRegs u = load_unit(plan.units + unit);
+
+  if (u.tag < 0) {
+    // ------------------------------------------------------ long-row chunk
+    Acc acc;
+    acc.zero();
+    S av[kSpmvItems];
+    IT cv[kSpmvItems];
+#pragma unroll
+    for (int k = 0; k < kSpmvItems; ++k) {
+      const int64_t i = u.s0 + k * 32 + lane;
+      if (i < u.s1) { av[k] = ld_stream(data + i); cv[k] = ld_stream(col + i); }
+    }
+    for (int64_t base = u.s0; base < u.s1; base += kSpmvBatch) {
+      S xv[kSpmvItems];
+#pragma unroll
+      for (int k = 0; k < kSpmvItems; ++k) {
+        if (base + k * 32 + lane < u.s1) xv[k] = ld_x(x + cv[k]);
+      }
+      // next batch's loads go out before this batch is summed
+      S an[kSpmvItems];
+      IT cn[kSpmvItems];
+      const int64_t nb = base + kSpmvBatch;
+#pragma unroll
+      for (int k = 0; k < kSpmvItems; ++k) {
+        const int64_t i = nb + k * 32 + lane;
+        if (i < u.s1) { an[k] = ld_stream(data + i); cn[k] = ld_stream(col + i); }
+      }
+#pragma unroll
+      for (int k = 0; k < kSpmvItems; ++k) {
+        if (base + k * 32 + lane < u.s1) acc.add_prod(av[k], xv[k]);
+      }
+#pragma unroll
+      for (int k = 0; k < kSpmvItems; ++k) { av[k] = an[k]; cv[k] = cn[k]; }
+    }
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1) acc.shfl_combine(m);
+    if (u.nch == 1) {
+      if (lane == 0) y[u.row] = acc.result();
+      return;
+    }
+    const int64_t u0 = unit + (u.tag + 1);  // first chunk of this row
+    R* part = static_cast<R*>(plan.partials);
+    int ticket = 0;
+    if (lane == 0) {
+      acc.store(part + unit * Acc::kPartialReals);
+      __threadfence();
+      ticket = atomicAdd(plan.counters + u0, 1);
+    }
+    ticket = __shfl_sync(0xffffffffu, ticket, 0);
+    if (ticket != u.nch - 1) return;
+    __threadfence();
+    Acc fin;
+    fin.zero();
+    for (int64_t c = lane; c < u.nch; c += 32) {
+      Acc p;
+      p.load_cg(part + (u0 + c) * Acc::kPartialReals);
+      fin.combine(p);
+    }
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1) fin.shfl_combine(m);
+    if (lane == 0) {
+      y[u.row] = fin.result();
+      plan.counters[u0] = 0;  // ready for the next call
+    }
+    return;
+  }
+
+  // -------------------------------------------------------------- row block
+  using SAcc = SpmvAcc<DT, SHORT_COMP>;
+  constexpr bool kLo = SAcc::kLo;
+  const int64_t r0 = u.row;
+  const int nr = u.tag - u.row;
+  const int n = static_cast<int>(u.s1 - u.s0);
+  unsigned char* wbase = smem_raw + warp * spmv_warp_smem_bytes<DT, SHORT_COMP>();
+  R* sh_hi = reinterpret_cast<R*>(wbase);
+  R* sh_lo = sh_hi + NC * kSpmvBatch;
+  int32_t* sh_off = reinterpret_cast<int32_t*>(sh_hi + NC * kSpmvBatch * (kLo ? 2 : 1));
+
+  S av[kSpmvItems];
+  IT cv[kSpmvItems];
+#pragma unroll
+  for (int k = 0; k < kSpmvItems; ++k) {
+    const int i = k * 32 + lane;
+    if (i < n) { av[k] = ld_stream(data + u.s0 + i); cv[k] = ld_stream(col + u.s0 + i); }
+  }
+  for (int i = lane; i <= nr; i += 32) sh_off[i] = static_cast<int32_t>(ld_ptr(ptr, r0 + i) - u.s0);
+#pragma unroll
+  for (int k = 0; k < kSpmvItems; ++k) {
+    const int i = k * 32 + lane;
+    if (i < n) {
+      R hi[NC], lo[NC];
+      SAcc::prod(av[k], ld_x(x + cv[k]), hi, lo);
+#pragma unroll
+      for (int q = 0; q < NC; ++q) {
+        sh_hi[q * kSpmvBatch + i] = hi[q];
+        if constexpr (kLo) sh_lo[q * kSpmvBatch + i] = lo[q];
+      }
+    }
+  }
+  __syncwarp();
+
+  // Lane-level merge path over the unit's merged list of L = nr row ends and
+  // n nonzeros: row i's end sits at position off[i+1] + i.  Lane l walks
+  // positions [l*K, (l+1)*K) -- every lane does the same number of steps,
+  // whatever the row lengths -- summing nonzeros and emitting a row at its end.
+  const int L = nr + n;
+  const int K = (L + 31) >> 5;
+  const int d = min(lane * K, L);
+  int lo_i = max(0, d - n), hi_i = min(d, nr);
+  while (lo_i < hi_i) {  // i = number of row ends before position d
+    const int mid = (lo_i + hi_i) >> 1;
+    if (sh_off[mid + 1] + mid < d) lo_i = mid + 1; else hi_i = mid;
+  }
+  int i = lo_i, j = d - lo_i;
+  const int stop = min(d + K, L);
+  int next_end = i < nr ? sh_off[i + 1] : 0x7fffffff;
+  SAcc acc, first;
+  acc.zero();
+  first.zero();
+  int first_row = -1;
+  for (int pos = d; pos < stop; ++pos) {
+    if (j >= next_end) {
+      if (first_row < 0) {
+        first_row = i;   // may continue a row begun by earlier lanes: finish after the scan
+        first = acc;
+      } else {
+        y[r0 + i] = acc.result();
+      }
+      acc.zero();
+      ++i;
+      next_end = i < nr ? sh_off[i + 1] : 0x7fffffff;
+    } else {
+      R hi[NC], lo[NC];
+#pragma unroll
+      for (int q = 0; q < NC; ++q) {
+        hi[q] = sh_hi[q * kSpmvBatch + j];
+        lo[q] = kLo ? sh_lo[q * kSpmvBatch + j] : R(0);
+      }
+      acc.add_rec(hi, lo);
+      ++j;
+    }
+  }
+  // The partial a lane holds at its end belongs to row i, which the next lane
+  // starts in.  A segmented inclusive scan over lanes (keys are non-decreasing
+  // row indices) totals the partials of rows spanning several lanes.
+  const int key = i;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    SAcc other = acc;
+    other.shfl_up(o);
+    const int okey = __shfl_up_sync(0xffffffffu, key, o);
+    if (lane >= o && okey == key) acc.combine(other);
+  }
+  SAcc carry = acc;
+  carry.shfl_up(1);
+  if (first_row >= 0) {
+    if (lane > 0) first.combine(carry);
+    y[r0 + first_row] = first.result();
+  }
+}
+
+template <int DT, typename IT, typename PT, bool SHORT_COMP>
+static int spmv_launch_mode(const void* data, const void* idx, const void* ptr, const void* x, void* y,
+                            const fsb_spmv_plan& plan, cudaStream_t st) {
+  using S = typename VT<DT>::Store;
+  const size_t smem = size_t(spmv_warp_smem_bytes<DT, SHORT_COMP>()) * kSpmvWarps;
+  auto kern = k_spmv_csr<DT, IT, PT, SHORT_COMP>;
+  if (smem > 48 * 1024) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+      return FSB_ERR_CUDA;
+  }
+  const int64_t blocks = ceil_div(plan.n_units, kSpmvWarps);
+  kern<<<(unsigned)blocks, kSpmvWarps * 32, smem, st>>>(static_cast<const S*>(data), static_cast<const IT*>(idx),
+                                                        static_cast<const PT*>(ptr), static_cast<const S*>(x),
+                                                        static_cast<S*>(y), plan);
+  FSB_LAUNCH_CHECK();
+  return FSB_OK;
+}
+
+template <int DT, typename IT, typename PT>
+static int spmv_launch(const void* data, const void* idx, const void* ptr, const void* x, void* y,
+                       const fsb_spmv_plan& plan, cudaStream_t st) {
+  if (plan.cap != kSpmvCap || plan.chunk_nnz % kSpmvBatch != 0) return FSB_ERR_INVALID_ARG;
+  if (plan.flags & FSB_SPMV_FAST_SHORT_ROWS) return spmv_launch_mode<DT, IT, PT, false>(data, idx, ptr, x, y, plan, st);
+  return spmv_launch_mode<DT, IT, PT, true>(data, idx, ptr, x, y, plan, st);
+}
+
+template <int DT>
+static int spmv_dispatch_idx(const void* data, const void* idx, int i64, const void* ptr, int p64, const void* x,
+                             void* y, const fsb_spmv_plan& plan, cudaStream_t st) {
+  if (i64) {
+    return p64 ? spmv_launch<DT, int64_t, int64_t>(data, idx, ptr, x, y, plan, st)
+               : spmv_launch<DT, int64_t, int32_t>(data, idx, ptr, x, y, plan, st);
+  }
+  return p64 ? spmv_launch<DT, int32_t, int64_t>(data, idx, ptr, x, y, plan, st)
+             : spmv_launch<DT, int32_t, int32_t>(data, idx, ptr, x, y, plan, st);
+}
+
+}  // namespace fsb
+
+using namespace fsb;
+
+extern "C" {
+
+int64_t fsb_spmv_partial_bytes(int dtype) {
+  switch (dtype) {
+    case FSB_F16: case FSB_BF16: case FSB_F32: return 2 * sizeof(float);
+    case FSB_F64: return 2 * sizeof(double);
+    case FSB_C64: return 4 * sizeof(float);
+    case FSB_C128: return 4 * sizeof(double);
+    default: return -1;
+  }
+}
+
+int fsb_spmv_csr(int dtype, const void* data, const void* indices, int idx_is_64, const void* indptr, int ptr_is_64,
+                 int64_t n_rows, int64_t n_cols, const void* x, void* y, const fsb_spmv_plan* plan, void* stream) {
+  if (!plan || n_rows < 0 || n_cols < 0) return FSB_ERR_INVALID_ARG;
+  if (n_rows == 0 || plan->n_units == 0) return FSB_OK;
+  if (!indptr || !y || !plan->units || plan->cap < 1 ||
+      plan->chunk_nnz < 1)
+    return FSB_ERR_INVALID_ARG;
+  if (plan->n_units >= INT32_MAX) return FSB_ERR_UNSUPPORTED;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  switch (dtype) {
+    case FSB_F16: return spmv_dispatch_idx<FSB_F16>(data, indices, idx_is_64, indptr, ptr_is_64, x, y, *plan, st);
+    case FSB_BF16: return spmv_dispatch_idx<FSB_BF16>(data, indices, idx_is_64, indptr, ptr_is_64, x, y, *plan, st);
+    case FSB_F32: return spmv_dispatch_idx<FSB_F32>(data, indices, idx_is_64, indptr, ptr_is_64, x, y, *plan, st);
+    case FSB_F64: return spmv_dispatch_idx<FSB_F64>(data, indices, idx_is_64, indptr, ptr_is_64, x, y, *plan, st);
+    case FSB_C64: return spmv_dispatch_idx<FSB_C64>(data, indices, idx_is_64, indptr, ptr_is_64, x, y, *plan, st);
+    case FSB_C128: return spmv_dispatch_idx<FSB_C128>(data, indices, idx_is_64, indptr, ptr_is_64, x, y, *plan, st);
+    default: return FSB_ERR_UNSUPPORTED;
+  }
+}
+
+}  // extern "C"

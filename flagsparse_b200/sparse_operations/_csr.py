@@ -1,0 +1,180 @@
+"""Native CSR plumbing shared by the SpMV / SpMM / SDDMM host code.
+
+Thin wrappers over the C ABI: inspection (one synchronising read instead of
+a chain of ``.item()`` calls), the stable transpose, stable row-length
+bucketing and the SpMV unit plan.  Device memory comes from torch; every
+computation runs in the native library.
+"""
+
+import ctypes
+
+import torch
+
+from .. import _native as nat
+
+
+def inspect_csr(indices, indptr, n_rows, nnz):
+    """Return a dict with indptr[0], indptr[-1], #decreasing steps, min/max column, max row length.
+
+    One kernel, one device-to-host read.
+    """
+    out = torch.empty(6, dtype=torch.int64, device=indptr.device)
+    if n_rows + 1 == 0:
+        raise ValueError("indptr must have at least one entry")
+    lib = nat.lib()
+    idx = indices if (indices is not None and nnz > 0) else None
+    nat.check(
+        lib.fsb_csr_inspect(
+            nat.ptr(idx), nat.is64(indices) if indices is not None else 0,
+            nat.ptr(indptr), nat.is64(indptr), int(n_rows), int(nnz),
+            nat.ptr(out), nat.stream_of(indptr.device),
+        ),
+        "fsb_csr_inspect",
+    )
+    v = out.tolist()
+    return {
+        "first": v[0],
+        "last": v[1],
+        "decreasing": v[2],
+        "min_col": v[3] if nnz > 0 else None,
+        "max_col": v[4] if nnz > 0 else None,
+        "max_row_nnz": v[5] if n_rows > 0 else 0,
+    }
+
+
+def transpose_pattern(indices, indptr, shape, out_index_dtype, out_indptr_dtype):
+    """Stable CSR transpose of the pattern.
+
+    Returns ``(t_indices, t_indptr, perm)`` where ``perm[k]`` is the source
+    position of transposed entry ``k``.  Identical to a stable argsort by
+    column followed by bincount/cumsum.
+    """
+    n_rows, n_cols = int(shape[0]), int(shape[1])
+    nnz = int(indices.numel())
+    device = indices.device
+    t_indices = torch.empty(nnz, dtype=out_index_dtype, device=device)
+    t_indptr = torch.empty(n_cols + 1, dtype=out_indptr_dtype, device=device)
+    perm = torch.empty(nnz, dtype=torch.int64, device=device)
+    lib = nat.lib()
+    ws_bytes = int(lib.fsb_csr_transpose_workspace_bytes(nnz, n_rows, n_cols)) if nnz > 0 else 0
+    if ws_bytes < 0:
+        raise RuntimeError("CSR transpose: nnz must be < 2^31")
+    ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=device)
+    nat.check(
+        lib.fsb_csr_transpose(
+            nat.ptr(indices), nat.is64(indices), nat.ptr(indptr), nat.is64(indptr),
+            n_rows, n_cols, nnz, nat.ptr(ws), ws_bytes,
+            nat.ptr(t_indices), 1 if out_index_dtype == torch.int64 else 0,
+            nat.ptr(t_indptr), 1 if out_indptr_dtype == torch.int64 else 0,
+            nat.ptr(perm), nat.stream_of(device),
+        ),
+        "fsb_csr_transpose",
+    )
+    return t_indices, t_indptr, perm
+
+
+def gather_values(values, perm, conj=False):
+    """values[perm] (conjugated for complex when ``conj``), computed natively."""
+    out = torch.empty(perm.numel(), dtype=values.dtype, device=values.device)
+    nat.check(
+        nat.lib().fsb_gather_values(
+            nat.dtype_code(values.dtype), nat.ptr(values), nat.ptr(perm), int(perm.numel()),
+            1 if conj else 0, nat.ptr(out), nat.stream_of(values.device),
+        ),
+        "fsb_gather_values",
+    )
+    return out
+
+
+def bucketize_rows(indptr, n_rows, upper_bounds):
+    """Stable row lists per row-length bucket.
+
+    ``upper_bounds[b]`` is the inclusive upper length of bucket ``b`` (``None``
+    = unbounded); bucket 0 includes empty rows.  Returns a list of int32
+    tensors (views into one buffer), one per bucket.
+    """
+    nb = len(upper_bounds)
+    device = indptr.device
+    rows = torch.empty(max(int(n_rows), 1), dtype=torch.int32, device=device)
+    counts = torch.zeros(nb, dtype=torch.int64, device=device)
+    ub = (ctypes.c_int64 * nb)(*[-1 if u is None else int(u) for u in upper_bounds])
+    lib = nat.lib()
+    ws_bytes = int(lib.fsb_csr_bucketize_workspace_bytes(int(n_rows), nb))
+    ws = torch.empty(max(ws_bytes, 8), dtype=torch.uint8, device=device)
+    nat.check(
+        lib.fsb_csr_bucketize(
+            nat.ptr(indptr), nat.is64(indptr), int(n_rows), ub, nb,
+            nat.ptr(ws), ws_bytes, nat.ptr(rows), nat.ptr(counts), nat.stream_of(device),
+        ),
+        "fsb_csr_bucketize",
+    )
+    out = []
+    off = 0
+    for c in counts.tolist():
+        out.append(rows[off:off + c])
+        off += c
+    return out
+
+
+class NativeSpmvPlan:
+    """Device arrays of the SpMV unit plan plus its scratch (see fsb_spmv_plan)."""
+
+    __slots__ = ("seg_row0", "seg_unit0", "units", "partials", "counters", "cap", "chunk_nnz",
+                 "n_segs", "n_units", "dtype", "flags", "_struct")
+
+    def __init__(self, indptr, n_rows, dtype, cap=None, chunk_nnz=None, fast_short_rows=False):
+        lib = nat.lib()
+        code = nat.dtype_code(dtype)
+        device = indptr.device
+        self.dtype = dtype
+        self.cap = int(cap) if cap is not None else int(lib.fsb_spmv_default_cap(code))
+        self.chunk_nnz = int(chunk_nnz) if chunk_nnz is not None else int(lib.fsb_spmv_default_chunk(code))
+        n_rows = int(n_rows)
+        st = nat.stream_of(device)
+        ws_bytes = int(lib.fsb_spmv_plan_workspace_bytes(n_rows))
+        ws = torch.empty(max(ws_bytes, 8), dtype=torch.uint8, device=device)
+        totals = torch.zeros(2, dtype=torch.int64, device=device)
+        if n_rows > 0:
+            nat.check(
+                lib.fsb_spmv_plan_analyze(nat.ptr(indptr), nat.is64(indptr), n_rows, self.cap,
+                                          self.chunk_nnz, nat.ptr(ws), ws_bytes, nat.ptr(totals), st),
+                "fsb_spmv_plan_analyze",
+            )
+        self.n_segs, self.n_units = (int(v) for v in totals.tolist())
+        self.seg_row0 = torch.empty(self.n_segs + 1, dtype=torch.int32, device=device)
+        self.seg_unit0 = torch.empty(self.n_segs + 1, dtype=torch.int32, device=device)
+        # fsb_spmv_unit: int64 nnz_begin, nnz_end; int32 row, tag, n_chunks, reserved (32 bytes)
+        self.units = torch.empty((max(self.n_units, 1), 4), dtype=torch.int64, device=device)
+        if n_rows > 0:
+            nat.check(
+                lib.fsb_spmv_plan_build(nat.ptr(indptr), nat.is64(indptr), n_rows, self.cap,
+                                        self.chunk_nnz, nat.ptr(ws), ws_bytes, nat.ptr(self.seg_row0),
+                                        nat.ptr(self.seg_unit0), nat.ptr(self.units), st),
+                "fsb_spmv_plan_build",
+            )
+        pbytes = int(lib.fsb_spmv_partial_bytes(code))
+        self.partials = torch.empty(max(self.n_units * pbytes, 16), dtype=torch.uint8, device=device)
+        self.counters = torch.zeros(max(self.n_units, 1), dtype=torch.int32, device=device)
+        self.flags = nat.FSB_SPMV_FAST_SHORT_ROWS if fast_short_rows else 0
+        self._struct = nat.SpmvPlan(
+            nat.ptr(self.seg_row0), nat.ptr(self.seg_unit0), nat.ptr(self.units),
+            self.n_segs, self.n_units, self.cap, self.chunk_nnz,
+            nat.ptr(self.partials), nat.ptr(self.counters), self.flags, 0,
+        )
+
+    def set_fast_short_rows(self, on):
+        self.flags = nat.FSB_SPMV_FAST_SHORT_ROWS if on else 0
+        self._struct.flags = self.flags
+
+    def struct_ref(self):
+        return ctypes.byref(self._struct)
+
+    def unit_table(self):
+        """Host copy of the unit descriptors as columns (begin, end, row, tag, n_chunks)."""
+        u = self.units[: self.n_units].cpu()
+        packed = u[:, 2]
+        row = (packed & 0xFFFFFFFF).to(torch.int64)
+        row = torch.where(row >= 2**31, row - 2**32, row)
+        tag = packed >> 32
+        nch = (u[:, 3] & 0xFFFFFFFF).to(torch.int64)
+        return u[:, 0].numpy(), u[:, 1].numpy(), row.numpy(), tag.numpy(), nch.numpy()

@@ -1,0 +1,174 @@
+/*
+ * flagsparse_b200 C ABI.
+ *
+ * Plain-C entry points of the sm_100a CSR SpMV / SpMM / SDDMM library.  Every
+ * function takes raw device pointers, sizes, dtype codes and a cudaStream_t
+ * passed as `void*`; none allocates device memory, none throws, none aborts.
+ * Each returns FSB_OK (0) or a negative FSB_ERR_* status.  Work is enqueued
+ * on `stream`; the functions return without synchronising unless stated.
+ *
+ * Every entry point names the flagos-ai/FlagSparse interface it replaces
+ * (paths relative to the FlagSparse source tree).  The Python host mirror in
+ * flagsparse_b200/sparse_operations binds these with ctypes.
+ */
+#ifndef FLAGSPARSE_B200_H_
+#define FLAGSPARSE_B200_H_
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define FSB_API __attribute__((visibility("default")))
+#else
+#define FSB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define FSB_OK 0
+#define FSB_ERR_INVALID_ARG (-1)   /* bad size, null pointer, bad enum          */
+#define FSB_ERR_UNSUPPORTED (-2)   /* dtype / index combination not built       */
+#define FSB_ERR_LAUNCH (-3)        /* kernel launch failed                      */
+#define FSB_ERR_TIMEOUT (-4)       /* a bounded device wait gave up             */
+#define FSB_ERR_CUDA (-5)          /* other CUDA runtime error                  */
+#define FSB_ERR_WORKSPACE (-6)     /* caller workspace too small                */
+
+/* ---- value dtype codes (torch dtype -> code mapping lives in _native.py) -- */
+#define FSB_F16 0
+#define FSB_BF16 1
+#define FSB_F32 2
+#define FSB_F64 3
+#define FSB_C64 4
+#define FSB_C128 5
+
+/* Library version (major*10000 + minor*100 + patch). */
+FSB_API int fsb_version(void);
+
+/* Human-readable text of a status code (static storage). */
+FSB_API const char* fsb_status_string(int status);
+
+/* ------------------------------------------------------------------------
+ * CSR inspection.  One pass over indptr and indices that gathers every fact
+ * the host-side validation needs, so the host reads one small vector instead
+ * of issuing a synchronising reduction per check.
+ * Replaces the chain of .item() checks in
+ *   sparse_operations/spmv_csr.py:569-586 (_prepare_spmv_csr_matrix),
+ *   sparse_operations/spmm_csr.py:371-403 (_prepare_spmm_csr_matrix),
+ *   sparse_operations/sddmm_csr.py:79-92 (_prepare_sddmm_csr_pattern).
+ * d_out (device, int64[6]) receives:
+ *   [0] indptr[0]  [1] indptr[n_rows]  [2] count of i with indptr[i+1] < indptr[i]
+ *   [3] min column index (INT64_MAX if nnz == 0)  [4] max column index (-1 if nnz == 0)
+ *   [5] max row length (0 if n_rows == 0)
+ * ------------------------------------------------------------------------ */
+FSB_API int fsb_csr_inspect(const void* indices, int idx_is_64, const void* indptr, int ptr_is_64,
+                    int64_t n_rows, int64_t nnz, int64_t* d_out, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Stable row-length bucketing.  Bucket b holds the rows whose length lies in
+ * (upper_bounds[b-1], upper_bounds[b]]; bucket 0 also holds empty rows and an
+ * upper bound < 0 means "no bound".  Rows of a bucket keep ascending order, so
+ * the result is identical to torch.nonzero on each bucket mask.
+ * Replaces _build_spmv_opt_buckets (sparse_operations/spmv_csr.py:371-417)
+ * and the count/compact kernels of sparse_operations/spmm_csr.py:3022-3153.
+ * rows_out: int32[n_rows], all buckets concatenated in bucket order.
+ * d_counts: int64[n_buckets] rows per bucket.  n_buckets <= 8.
+ * ------------------------------------------------------------------------ */
+FSB_API int64_t fsb_csr_bucketize_workspace_bytes(int64_t n_rows, int n_buckets);
+FSB_API int fsb_csr_bucketize(const void* indptr, int ptr_is_64, int64_t n_rows,
+                      const int64_t* upper_bounds, int n_buckets,
+                      void* workspace, int64_t workspace_bytes,
+                      int32_t* rows_out, int64_t* d_counts, void* stream);
+
+/* ------------------------------------------------------------------------
+ * CSR transpose (CSR of A -> CSR of A^T), stable in the original nonzero
+ * order, so entries of one transposed row keep ascending source-row order.
+ * Bit-identical to _transpose_csr_for_spmv (sparse_operations/spmv_csr.py:498-536)
+ * and _transpose_csr_for_spmm (sparse_operations/spmm_csr.py:407-445), which
+ * use a stable argsort by column, bincount and cumsum.
+ * perm (int64[nnz]) receives, for every transposed entry, the position of its
+ * value in the source arrays; fsb_gather_values applies it to any values.
+ * Requires nnz < 2^31 and n_cols < 2^32.
+ * ------------------------------------------------------------------------ */
+FSB_API int64_t fsb_csr_transpose_workspace_bytes(int64_t nnz, int64_t n_rows, int64_t n_cols);
+FSB_API int fsb_csr_transpose(const void* indices, int idx_is_64, const void* indptr, int ptr_is_64,
+                      int64_t n_rows, int64_t n_cols, int64_t nnz,
+                      void* workspace, int64_t workspace_bytes,
+                      void* t_indices, int t_idx_is_64, void* t_indptr, int t_ptr_is_64,
+                      int64_t* perm, void* stream);
+
+/* dst[i] = src[perm[i]] (conjugated when conj != 0 and dtype is complex). */
+FSB_API int fsb_gather_values(int dtype, const void* src, const int64_t* perm, int64_t n, int conj,
+                      void* dst, void* stream);
+
+/* ------------------------------------------------------------------------
+ * CSR SpMV  y = A x.
+ *
+ * A launch plan splits the matrix into work units of one warp each:
+ *  - row-block units: maximal runs of rows whose (row index + first nonzero
+ *    index) falls in one window of `cap`; every row of the run has at most
+ *    `cap` nonzeros, so a unit holds <= cap rows and < 2*cap nonzeros.  The
+ *    warp streams them with coalesced loads, parks the products in shared
+ *    memory and reduces each row with a team of lanes;
+ *  - long-row units: a row with more than `cap` nonzeros is cut into chunks of
+ *    `chunk_nnz` nonzeros; a row of one chunk is finished by its warp, a row of
+ *    several chunks leaves one partial sum per chunk in `partials` and the
+ *    warp that finishes last (per-row ticket) adds them in chunk order.
+ * All sums use compensated (Dot2) accumulation in the value's real type, so
+ * results do not depend on the unit split.
+ * Replaces _triton_spmv_csr_impl_prepared / _spmv_csr_real_kernel
+ * (sparse_operations/spmv_csr.py:702-746, 179-240) and the bucketed
+ * _triton_spmv_csr_impl_opt_prepared (spmv_csr.py:433-482).
+ * ------------------------------------------------------------------------ */
+typedef struct fsb_spmv_unit {
+  int64_t nnz_begin;         /* first nonzero of the unit                              */
+  int64_t nnz_end;           /* one past its last nonzero                              */
+  int32_t row;               /* first row (row block) / the row (long-row chunk)       */
+  int32_t tag;               /* >= 0: row block ending before row `tag`;
+                                < 0: chunk -(tag+1) of a long row                      */
+  int32_t n_chunks;          /* chunks of that long row (1 for row blocks)             */
+  int32_t reserved;
+} fsb_spmv_unit;
+
+typedef struct fsb_spmv_plan {
+  const int32_t* seg_row0;   /* [n_segs + 1] first row of each segment; last entry == n_rows */
+  const int32_t* seg_unit0;  /* [n_segs + 1] first work unit of each segment                */
+  const fsb_spmv_unit* units;/* [n_units]    unit descriptors                                */
+  int64_t n_segs;
+  int64_t n_units;
+  int32_t cap;               /* row-block window, see above                                  */
+  int32_t chunk_nnz;         /* nonzeros per long-row chunk                                  */
+  void* partials;            /* scratch: n_units * fsb_spmv_partial_bytes(dtype) bytes       */
+  int32_t* counters;         /* scratch: n_units int32, zero before the first call; every
+                                call leaves them zero again                                  */
+  int32_t flags;             /* FSB_SPMV_* bits                                              */
+  int32_t reserved;
+} fsb_spmv_plan;
+
+/* Sum the rows of row-block units (rows of <= cap nonzeros) with plain
+ * accumulation in the value's real type instead of Dot2.  Long rows stay
+ * compensated.  Off by default. */
+#define FSB_SPMV_FAST_SHORT_ROWS 1
+
+FSB_API int32_t fsb_spmv_default_cap(int dtype);
+FSB_API int32_t fsb_spmv_default_chunk(int dtype);
+FSB_API int64_t fsb_spmv_partial_bytes(int dtype);
+FSB_API int64_t fsb_spmv_plan_workspace_bytes(int64_t n_rows);
+/* d_totals (device int64[2]) receives n_segs and n_units. */
+FSB_API int fsb_spmv_plan_analyze(const void* indptr, int ptr_is_64, int64_t n_rows, int32_t cap,
+                          int32_t chunk_nnz, void* workspace, int64_t workspace_bytes,
+                          int64_t* d_totals, void* stream);
+FSB_API int fsb_spmv_plan_build(const void* indptr, int ptr_is_64, int64_t n_rows, int32_t cap,
+                        int32_t chunk_nnz, const void* workspace, int64_t workspace_bytes,
+                        int32_t* seg_row0, int32_t* seg_unit0, fsb_spmv_unit* units, void* stream);
+
+FSB_API int fsb_spmv_csr(int dtype, const void* data, const void* indices, int idx_is_64,
+                 const void* indptr, int ptr_is_64, int64_t n_rows, int64_t n_cols,
+                 const void* x, void* y, const fsb_spmv_plan* plan, void* stream);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif  /* FLAGSPARSE_B200_H_ */

@@ -1,0 +1,232 @@
+"""Generate golden vectors by running FlagSparse's own code on small seeded inputs.
+
+Runs only where the FlagSparse source tree is available (pass its ``src``
+directory as argv[1]); the committed ``*.npz`` files are what the tests read.
+The Triton kernels run on the CPU under ``TRITON_INTERPRET=1``.  FlagSparse's
+public entry points insist on CUDA tensors, so this script calls the same
+internal functions they call (prepare logic restated line by line where it
+only validates), e.g. ``_transpose_csr_for_spmv``, ``_build_spmv_opt_buckets``,
+``_triton_spmv_csr_impl_prepared``, ``_triton_spmm_csr_impl`` and
+``_run_sddmm_prepared``.
+
+Usage:  python tests/golden/make_golden.py <FlagSparse>/src
+"""
+
+import os
+import sys
+
+os.environ["TRITON_INTERPRET"] = "1"
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from flagsparse_b200 import workloads  # noqa: E402
+
+TORCH_DT = {
+    "float16": torch.float16,
+    "bfloat16": torch.bfloat16,
+    "float32": torch.float32,
+    "float64": torch.float64,
+    "complex64": torch.complex64,
+    "complex128": torch.complex128,
+}
+
+
+def np_of(t):
+    t = t.detach().cpu()
+    if t.dtype in (torch.float16, torch.bfloat16):
+        return t.to(torch.float32).numpy()
+    return t.numpy()
+
+
+def rand_vec(rng, n, dtype):
+    if dtype.is_complex:
+        v = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+        return torch.from_numpy(v).to(dtype)
+    return torch.from_numpy(rng.standard_normal(n)).to(dtype)
+
+
+def ref_prepared_spmv(m, data, indices, indptr, shape, op):
+    """FlagSparse prepare_spmv_csr (spmv_csr.py:614-687) minus the CUDA checks."""
+    op_code = m._normalize_spmv_op(op)
+    if m._spmv_op_transposes(op_code):
+        if op_code == m.SPMV_OP_CONJ_TRANS and data.dtype.is_complex:
+            data = data.conj().resolve_conj()
+        data, indices, indptr, shape = m._transpose_csr_for_spmv(data, indices, indptr, shape)
+    n_rows, n_cols = int(shape[0]), int(shape[1])
+    row_lengths = indptr[1:] - indptr[:-1]
+    max_row_nnz = int(row_lengths.max().item()) if n_rows > 0 else 0
+    block_nnz = 256
+    max_segments = max((max_row_nnz + block_nnz - 1) // block_nnz, 1)
+    while max_segments > 2048 and block_nnz < 65536:
+        block_nnz *= 2
+        max_segments = max((max_row_nnz + block_nnz - 1) // block_nnz, 1)
+    return m.PreparedCsrSpmv(
+        data=data.contiguous(), kernel_indices=indices.contiguous(), kernel_indptr=indptr.contiguous(),
+        shape=shape, n_rows=n_rows, n_cols=n_cols, block_nnz=block_nnz, max_segments=max_segments,
+        opt_max_segments=None, row_lengths=row_lengths, max_row_nnz=max_row_nnz, op=op_code,
+    )
+
+
+def spmv_cases(m, out):
+    rng = np.random.Generator(np.random.PCG64(101))
+    mats = {
+        "small": workloads.mask_csr(40, 56, seed=11, dtype=np.float64),
+        "wide": workloads.mask_csr(24, 5000, seed=12, dtype=np.float64, density=0.002, long_rows=(5,)),
+    }
+    for mname, mat in mats.items():
+        out[f"spmv_{mname}_indptr"] = mat["indptr"]
+        out[f"spmv_{mname}_indices"] = mat["indices"]
+        out[f"spmv_{mname}_shape"] = np.array(mat["shape"])
+        base = mat["data"]
+        base_c = base + 1j * rng.standard_normal(base.size)
+        out[f"spmv_{mname}_data_real"] = base
+        out[f"spmv_{mname}_data_cplx"] = base_c
+        for dname, dt in TORCH_DT.items():
+            for op in ("non", "trans", "conj"):
+                if op == "conj" and not dt.is_complex:
+                    continue
+                src = base_c if dt.is_complex else base
+                data = torch.from_numpy(src).to(dt)
+                indices = torch.from_numpy(mat["indices"]).to(torch.int32)
+                indptr = torch.from_numpy(mat["indptr"]).to(torch.int64)
+                p = ref_prepared_spmv(m, data, indices, indptr, mat["shape"], op)
+                x = rand_vec(rng, p.n_cols, dt)
+                y = m._triton_spmv_csr_impl_prepared(p, x)
+                key = f"spmv_{mname}_{dname}_{op}"
+                out[key + "_x"] = np_of(x)
+                out[key + "_y"] = np_of(y)
+                if dt in (torch.float32, torch.float64) and op == "non":
+                    buckets = m._build_spmv_opt_buckets(
+                        p.row_lengths, p.max_row_nnz, torch.int32, fp64=dt == torch.float64
+                    )
+                    yo = m._triton_spmv_csr_impl_opt_prepared(p, x, opt_buckets=buckets)
+                    out[key + "_yopt"] = np_of(yo)
+                    out[key + "_nbuckets"] = np.array(len(buckets))
+                    for b, bucket in enumerate(buckets):
+                        out[key + f"_bucket{b}_rows"] = bucket["rows"].numpy()
+                        out[key + f"_bucket{b}_max_segs"] = np.array(bucket["max_segs"])
+
+
+def config1_case(m, out):
+    c = workloads.poisson_csr()
+    data = torch.from_numpy(c["data"])
+    p = ref_prepared_spmv(m, data, torch.from_numpy(c["indices"]), torch.from_numpy(c["indptr"]), c["shape"], "non")
+    y = m._triton_spmv_csr_impl_prepared(p, torch.from_numpy(c["x"]))
+    out["config1_f32_y"] = np_of(y)
+    out["config1_nnz"] = np.array(c["indices"].size)
+
+
+def transpose_cases(m, out):
+    rng = np.random.Generator(np.random.PCG64(7))
+    # unsorted columns with duplicates and empty rows: stability matters
+    n_rows, n_cols, nnz = 30, 17, 140
+    rows = np.sort(rng.integers(0, n_rows, nnz))
+    rows[rows == 4] = 5  # row 4 empty
+    indptr = np.zeros(n_rows + 1, dtype=np.int64)
+    np.cumsum(np.bincount(rows, minlength=n_rows), out=indptr[1:])
+    cols = rng.integers(0, n_cols - 2, nnz).astype(np.int32)  # last two columns empty
+    data = rng.standard_normal(nnz)
+    for idx_dt, ptr_dt, tag in ((torch.int32, torch.int64, "i32p64"), (torch.int64, torch.int32, "i64p32")):
+        td, ti, tp, shape = m._transpose_csr_for_spmv(
+            torch.from_numpy(data), torch.from_numpy(cols).to(idx_dt), torch.from_numpy(indptr).to(ptr_dt),
+            (n_rows, n_cols),
+        )
+        out[f"transpose_{tag}_data"] = td.numpy()
+        out[f"transpose_{tag}_indices"] = ti.numpy()
+        out[f"transpose_{tag}_indptr"] = tp.numpy()
+        out[f"transpose_{tag}_indices_dtype"] = np.array(str(ti.dtype))
+        out[f"transpose_{tag}_indptr_dtype"] = np.array(str(tp.dtype))
+    out["transpose_src_indptr"] = indptr
+    out["transpose_src_indices"] = cols
+    out["transpose_src_data"] = data
+    out["transpose_shape"] = np.array((n_rows, n_cols))
+
+
+def spmm_cases(sm, out):
+    rng = np.random.Generator(np.random.PCG64(202))
+    for (M, K, N, seed) in ((64, 96, 16, 21), (40, 30, 5, 22), (33, 3000, 64, 23)):
+        mat = workloads.mask_csr(M, K, seed=seed, dtype=np.float64,
+                                 density=0.004 if K > 1000 else None, long_rows=(2,) if K > 1000 else ())
+        tag = f"spmm_{M}x{K}x{N}"
+        out[tag + "_indptr"] = mat["indptr"]
+        out[tag + "_indices"] = mat["indices"]
+        base = mat["data"]
+        base_c = base + 1j * rng.standard_normal(base.size)
+        out[tag + "_data_real"] = base
+        out[tag + "_data_cplx"] = base_c
+        for dname in ("float32", "float64", "complex64"):
+            dt = TORCH_DT[dname]
+            data = torch.from_numpy(base_c if dt.is_complex else base).to(dt)
+            if dt.is_complex:
+                B = torch.from_numpy(rng.standard_normal((K, N)) + 1j * rng.standard_normal((K, N))).to(dt)
+            else:
+                B = torch.from_numpy(rng.standard_normal((K, N))).to(dt)
+            indices = torch.from_numpy(mat["indices"]).to(torch.int32)
+            indptr = torch.from_numpy(mat["indptr"]).to(torch.int64)
+            max_row = int((indptr[1:] - indptr[:-1]).max().item())
+            launch = sm._resolve_spmm_base_triton_launch(dt, N, max_row)
+            C = sm._triton_spmm_csr_impl(
+                data, indices, indptr, B, M, N, block_n=launch["block_n"], block_nnz=launch["block_nnz"],
+                num_warps=launch["num_warps"], num_stages=launch["num_stages"],
+            )
+            out[f"{tag}_{dname}_B"] = np_of(B)
+            out[f"{tag}_{dname}_C"] = np_of(C)
+
+
+def sddmm_cases(dm, out):
+    rng = np.random.Generator(np.random.PCG64(303))
+    for (M, N, K, seed) in ((8, 10, 8, 31), (64, 96, 16, 32), (50, 40, 37, 33)):
+        mat = workloads.mask_csr(M, N, seed=seed, dtype=np.float64)
+        tag = f"sddmm_{M}x{N}x{K}"
+        out[tag + "_indptr"] = mat["indptr"]
+        out[tag + "_indices"] = mat["indices"]
+        for dname in ("float32", "float64"):
+            dt = TORCH_DT[dname]
+            x = torch.from_numpy(rng.standard_normal((M, K)) * 0.125).to(dt)
+            y = torch.from_numpy(rng.standard_normal((N, K)) * 0.125).to(dt)
+            data = torch.from_numpy(mat["data"]).to(dt)
+            indices = torch.from_numpy(mat["indices"]).to(torch.int32)
+            indptr = torch.from_numpy(mat["indptr"]).to(torch.int64)
+            row_ids = dm._build_row_ids(indptr)
+            bk, nw = dm._resolve_sddmm_launch_config(K)
+            p = dm.SDDMMPrepared(indices=indices, indptr=indptr, shape=(M, N), row_ids=row_ids, block_k=bk,
+                                 num_warps=nw)
+            res, _meta = dm._run_sddmm_prepared(p, x, y, data, 1.25, 0.5, None)
+            out[f"{tag}_{dname}_x"] = x.numpy()
+            out[f"{tag}_{dname}_y"] = y.numpy()
+            out[f"{tag}_{dname}_data"] = data.numpy()
+            out[f"{tag}_{dname}_out"] = res.numpy()
+
+
+def main():
+    src = sys.argv[1] if len(sys.argv) > 1 else None
+    if not src or not os.path.isdir(src):
+        raise SystemExit("usage: make_golden.py <FlagSparse>/src")
+    sys.path.insert(0, src)
+    from flagsparse.sparse_operations import sddmm_csr as dm
+    from flagsparse.sparse_operations import spmm_csr as sm
+    from flagsparse.sparse_operations import spmv_csr as m
+
+    torch.manual_seed(0)
+    groups = {
+        "golden_spmv.npz": lambda o: (spmv_cases(m, o), transpose_cases(m, o)),
+        "golden_config1.npz": lambda o: config1_case(m, o),
+        "golden_spmm.npz": lambda o: spmm_cases(sm, o),
+        "golden_sddmm.npz": lambda o: sddmm_cases(dm, o),
+    }
+    only = set(sys.argv[2:])
+    for fname, fn in groups.items():
+        if only and fname not in only:
+            continue
+        out = {}
+        fn(out)
+        np.savez_compressed(os.path.join(HERE, fname), **out)
+        print(fname, len(out), "arrays")
+
+
+if __name__ == "__main__":
+    main()
