@@ -47,6 +47,7 @@ class SpmvPlan(ctypes.Structure):
         ("units", _c_ptr),
         ("n_segs", _c_i64),
         ("n_units", _c_i64),
+        ("n_slots", _c_i64),
         ("cap", _c_i32),
         ("chunk_nnz", _c_i32),
         ("partials", _c_ptr),

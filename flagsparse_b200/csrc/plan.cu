@@ -74,13 +74,14 @@ static int inspect_impl(const void* idx, const void* ptr, int64_t n_rows, int64_
 // a long row, is row 0, or when its window key (ptr[r] + r) / cap differs from
 // the previous row's.  A long segment is one row and owns ceil(len/chunk)
 // units; every other segment owns one unit.  Channel 0 counts segments,
-// channel 1 counts units.
+// channel 1 units, channel 2 scratch slots (one per chunk of a row of two or
+// more chunks: only those chunks publish a partial sum).
 // ---------------------------------------------------------------------------
 template <typename PT>
 struct SpmvSegFlags {
   const PT* ptr;
   int64_t cap, chunk;
-  __device__ __forceinline__ Vec<2> operator()(int64_t r) const {
+  __device__ __forceinline__ Vec<3> operator()(int64_t r) const {
     int64_t a = ld_ptr(ptr, r), b = ld_ptr(ptr, r + 1);
     int64_t len = b - a;
     bool is_long = len > cap;
@@ -92,20 +93,41 @@ struct SpmvSegFlags {
       bool prev_long = (a - pa) > cap;
       start = prev_long || ((pa + r - 1) / cap != (a + r) / cap);
     }
-    Vec<2> v;
+    const int64_t nch = is_long ? ceil_div(len, chunk) : 0;
+    Vec<3> v;
     v.v[0] = start ? 1 : 0;
-    v.v[1] = is_long ? ceil_div(len, chunk) : (start ? 1 : 0);
+    v.v[1] = is_long ? nch : (start ? 1 : 0);
+    v.v[2] = nch > 1 ? nch : 0;
     return v;
   }
 };
 
+// Records every segment start and writes the chunk descriptors of long rows
+// (k_spmv_units writes the row-block descriptors).
+template <typename PT>
 struct SpmvSegWriter {
+  const PT* ptr;
+  int64_t cap, chunk;
   int32_t* seg_row0;
   int32_t* seg_unit0;
-  __device__ __forceinline__ void operator()(int64_t r, const Vec<2>& pre, const Vec<2>& val) const {
+  fsb_spmv_unit* units;
+  __device__ __forceinline__ void operator()(int64_t r, const Vec<3>& pre, const Vec<3>& val) const {
     if (val.v[0] == 0) return;
     seg_row0[pre.v[0]] = static_cast<int32_t>(r);
     seg_unit0[pre.v[0]] = static_cast<int32_t>(pre.v[1]);
+    const int64_t a = ld_ptr(ptr, r), len = ld_ptr(ptr, r + 1) - a;
+    if (len <= cap) return;
+    const int32_t nch = static_cast<int32_t>(val.v[1]);
+    for (int32_t k = 0; k < nch; ++k) {
+      fsb_spmv_unit d;
+      d.nnz_begin = a + int64_t(k) * chunk;
+      d.nnz_end = min(a + int64_t(k + 1) * chunk, a + len);
+      d.row = static_cast<int32_t>(r);
+      d.tag = -(k + 1);
+      d.n_chunks = nch;
+      d.slot = nch > 1 ? static_cast<int32_t>(pre.v[2] + k) : -1;
+      units[pre.v[1] + k] = d;
+    }
   }
 };
 
@@ -114,38 +136,39 @@ __global__ void k_spmv_plan_sentinel(const int64_t* totals, int64_t n_rows, int3
   seg_unit0[totals[0]] = static_cast<int32_t>(totals[1]);
 }
 
-// One thread per segment writes the descriptors of the segment's units.
+// One thread per row-block segment writes that segment's descriptor.
 template <typename PT>
 __global__ void k_spmv_units(const PT* ptr, const int64_t* totals, const int32_t* seg_row0, const int32_t* seg_unit0,
-                             int64_t cap, int64_t chunk, fsb_spmv_unit* units) {
+                             int64_t cap, fsb_spmv_unit* units) {
   const int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (s >= totals[0]) return;
   const int32_t r0 = seg_row0[s], r1 = seg_row0[s + 1];
-  const int32_t u0 = seg_unit0[s], u1 = seg_unit0[s + 1];
   const int64_t a = ld_ptr(ptr, r0);
-  const int64_t len0 = ld_ptr(ptr, r0 + 1) - a;
-  if (r1 - r0 == 1 && len0 > cap) {
-    const int32_t nch = u1 - u0;
-    for (int32_t k = 0; k < nch; ++k) {
-      fsb_spmv_unit d;
-      d.nnz_begin = a + int64_t(k) * chunk;
-      d.nnz_end = min(a + int64_t(k + 1) * chunk, a + len0);
-      d.row = r0;
-      d.tag = -(k + 1);
-      d.n_chunks = nch;
-      d.reserved = 0;
-      units[u0 + k] = d;
-    }
-  } else {
-    fsb_spmv_unit d;
-    d.nnz_begin = a;
-    d.nnz_end = ld_ptr(ptr, r1);
-    d.row = r0;
-    d.tag = r1;
-    d.n_chunks = 1;
-    d.reserved = 0;
-    units[u0] = d;
-  }
+  if (r1 - r0 == 1 && ld_ptr(ptr, r0 + 1) - a > cap) return;  // long row: written by the scan
+  fsb_spmv_unit d;
+  d.nnz_begin = a;
+  d.nnz_end = ld_ptr(ptr, r1);
+  d.row = r0;
+  d.tag = r1;
+  d.n_chunks = 1;
+  d.slot = -1;
+  units[seg_unit0[s]] = d;
+}
+
+template <typename PT>
+static int spmv_plan_build_impl(const PT* ptr, int64_t n_rows, int64_t cap, int64_t chunk, const int64_t* ws,
+                                int32_t* seg_row0, int32_t* seg_unit0, fsb_spmv_unit* units, cudaStream_t st) {
+  const int64_t* totals = scan_totals<3>(ws, n_rows);
+  int rc = scan_apply<3>(SpmvSegFlags<PT>{ptr, cap, chunk}, SpmvSegWriter<PT>{ptr, cap, chunk, seg_row0, seg_unit0, units},
+                         n_rows, ws, st);
+  if (rc != FSB_OK) return rc;
+  k_spmv_plan_sentinel<<<1, 1, 0, st>>>(totals, n_rows, seg_row0, seg_unit0);
+  FSB_LAUNCH_CHECK();
+  // at most one segment per row
+  const unsigned blocks = (unsigned)ceil_div(n_rows > 0 ? n_rows : 1, 256);
+  k_spmv_units<PT><<<blocks, 256, 0, st>>>(ptr, totals, seg_row0, seg_unit0, cap, units);
+  FSB_LAUNCH_CHECK();
+  return FSB_OK;
 }
 
 __global__ void k_copy_totals(const int64_t* src, int64_t* dst, int n) {
@@ -344,7 +367,7 @@ int32_t fsb_spmv_default_cap(int dtype) { (void)dtype; return 128; }
 // Long rows are cut into chunks of two 256-nonzero batches per warp.
 int32_t fsb_spmv_default_chunk(int dtype) { (void)dtype; return 512; }
 
-int64_t fsb_spmv_plan_workspace_bytes(int64_t n_rows) { return scan_workspace_bytes<2>(n_rows); }
+int64_t fsb_spmv_plan_workspace_bytes(int64_t n_rows) { return scan_workspace_bytes<3>(n_rows); }
 
 int fsb_spmv_plan_analyze(const void* indptr, int ptr_is_64, int64_t n_rows, int32_t cap, int32_t chunk_nnz,
                           void* workspace, int64_t workspace_bytes, int64_t* d_totals, void* stream) {
@@ -355,12 +378,12 @@ int fsb_spmv_plan_analyze(const void* indptr, int ptr_is_64, int64_t n_rows, int
   int64_t* ws = static_cast<int64_t*>(workspace);
   int rc;
   if (ptr_is_64) {
-    rc = scan_analyze<2>(SpmvSegFlags<int64_t>{static_cast<const int64_t*>(indptr), cap, chunk_nnz}, n_rows, ws, st);
+    rc = scan_analyze<3>(SpmvSegFlags<int64_t>{static_cast<const int64_t*>(indptr), cap, chunk_nnz}, n_rows, ws, st);
   } else {
-    rc = scan_analyze<2>(SpmvSegFlags<int32_t>{static_cast<const int32_t*>(indptr), cap, chunk_nnz}, n_rows, ws, st);
+    rc = scan_analyze<3>(SpmvSegFlags<int32_t>{static_cast<const int32_t*>(indptr), cap, chunk_nnz}, n_rows, ws, st);
   }
   if (rc != FSB_OK) return rc;
-  k_copy_totals<<<1, 32, 0, st>>>(scan_totals<2>(ws, n_rows), d_totals, 2);
+  k_copy_totals<<<1, 32, 0, st>>>(scan_totals<3>(ws, n_rows), d_totals, 3);
   FSB_LAUNCH_CHECK();
   return FSB_OK;
 }
@@ -373,28 +396,11 @@ int fsb_spmv_plan_build(const void* indptr, int ptr_is_64, int64_t n_rows, int32
   if (workspace_bytes < fsb_spmv_plan_workspace_bytes(n_rows)) return FSB_ERR_WORKSPACE;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int64_t* ws = static_cast<const int64_t*>(workspace);
-  const int64_t* totals = scan_totals<2>(ws, n_rows);
-  SpmvSegWriter w{seg_row0, seg_unit0};
-  int rc;
-  if (ptr_is_64) {
-    rc = scan_apply<2>(SpmvSegFlags<int64_t>{static_cast<const int64_t*>(indptr), cap, chunk_nnz}, w, n_rows, ws, st);
-  } else {
-    rc = scan_apply<2>(SpmvSegFlags<int32_t>{static_cast<const int32_t*>(indptr), cap, chunk_nnz}, w, n_rows, ws, st);
-  }
-  if (rc != FSB_OK) return rc;
-  k_spmv_plan_sentinel<<<1, 1, 0, st>>>(totals, n_rows, seg_row0, seg_unit0);
-  FSB_LAUNCH_CHECK();
-  // at most one segment per row
-  const unsigned blocks = (unsigned)ceil_div(n_rows > 0 ? n_rows : 1, 256);
-  if (ptr_is_64) {
-    k_spmv_units<int64_t><<<blocks, 256, 0, st>>>(static_cast<const int64_t*>(indptr), totals, seg_row0, seg_unit0,
-                                                  cap, chunk_nnz, units);
-  } else {
-    k_spmv_units<int32_t><<<blocks, 256, 0, st>>>(static_cast<const int32_t*>(indptr), totals, seg_row0, seg_unit0,
-                                                  cap, chunk_nnz, units);
-  }
-  FSB_LAUNCH_CHECK();
-  return FSB_OK;
+  if (ptr_is_64)
+    return spmv_plan_build_impl(static_cast<const int64_t*>(indptr), n_rows, cap, chunk_nnz, ws, seg_row0, seg_unit0,
+                                units, st);
+  return spmv_plan_build_impl(static_cast<const int32_t*>(indptr), n_rows, cap, chunk_nnz, ws, seg_row0, seg_unit0,
+                              units, st);
 }
 
 int64_t fsb_csr_bucketize_workspace_bytes(int64_t n_rows, int n_buckets) {

@@ -184,7 +184,7 @@ constexpr int kSpmvItems = 8;     // nonzeros per lane per batch
 constexpr int kSpmvBatch = 32 * kSpmvItems;
 constexpr int kSpmvCap = kSpmvBatch / 2;  // row-block window: n < 2*cap <= batch
 
-struct UnitRegs { int64_t s0, s1; int32_t row, tag, nch; };
+struct UnitRegs { int64_t s0, s1; int32_t row, tag, nch, slot; };
 
 __device__ __forceinline__ UnitRegs load_unit(const fsb_spmv_unit* u) {
   const int4* p = reinterpret_cast<const int4*>(u);
@@ -195,6 +195,7 @@ __device__ __forceinline__ UnitRegs load_unit(const fsb_spmv_unit* u) {
   r.row = b.x;
   r.tag = b.y;
   r.nch = b.z;
+  r.slot = b.w;
   return r;
 }
 
@@ -268,13 +269,13 @@ k_spmv_csr(const typename VT<DT>::Store* __restrict__ data, const IT* __restrict
       if (lane == 0) y[u.row] = acc.result();
       return;
     }
-    const int64_t u0 = unit + (u.tag + 1);  // first chunk of this row
+    const int64_t s0 = int64_t(u.slot) + (u.tag + 1);  // slot of this row's first chunk
     R* part = static_cast<R*>(plan.partials);
     int ticket = 0;
     if (lane == 0) {
-      acc.store(part + unit * Acc::kPartialReals);
+      acc.store(part + int64_t(u.slot) * Acc::kPartialReals);
       __threadfence();
-      ticket = atomicAdd(plan.counters + u0, 1);
+      ticket = atomicAdd(plan.counters + s0, 1);
     }
     ticket = __shfl_sync(0xffffffffu, ticket, 0);
     if (ticket != u.nch - 1) return;
@@ -283,14 +284,14 @@ k_spmv_csr(const typename VT<DT>::Store* __restrict__ data, const IT* __restrict
     fin.zero();
     for (int64_t c = lane; c < u.nch; c += 32) {
       Acc p;
-      p.load_cg(part + (u0 + c) * Acc::kPartialReals);
+      p.load_cg(part + (s0 + c) * Acc::kPartialReals);
       fin.combine(p);
     }
 #pragma unroll
     for (int m = 16; m > 0; m >>= 1) fin.shfl_combine(m);
     if (lane == 0) {
       y[u.row] = fin.result();
-      plan.counters[u0] = 0;  // ready for the next call
+      plan.counters[s0] = 0;  // ready for the next call
     }
     return;
   }
@@ -446,8 +447,8 @@ int fsb_spmv_csr(int dtype, const void* data, const void* indices, int idx_is_64
                  int64_t n_rows, int64_t n_cols, const void* x, void* y, const fsb_spmv_plan* plan, void* stream) {
   if (!plan || n_rows < 0 || n_cols < 0) return FSB_ERR_INVALID_ARG;
   if (n_rows == 0 || plan->n_units == 0) return FSB_OK;
-  if (!indptr || !y || !plan->units || plan->cap < 1 ||
-      plan->chunk_nnz < 1)
+  if (!indptr || !y || !plan->units || plan->cap < 1 || plan->chunk_nnz < 1 || plan->n_slots < 0 ||
+      (plan->n_slots > 0 && (!plan->partials || !plan->counters)))
     return FSB_ERR_INVALID_ARG;
   if (plan->n_units >= INT32_MAX) return FSB_ERR_UNSUPPORTED;
   cudaStream_t st = static_cast<cudaStream_t>(stream);

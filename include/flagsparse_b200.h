@@ -113,8 +113,9 @@ FSB_API int fsb_gather_values(int dtype, const void* src, const int64_t* perm, i
  *    memory and reduces each row with a team of lanes;
  *  - long-row units: a row with more than `cap` nonzeros is cut into chunks of
  *    `chunk_nnz` nonzeros; a row of one chunk is finished by its warp, a row of
- *    several chunks leaves one partial sum per chunk in `partials` and the
- *    warp that finishes last (per-row ticket) adds them in chunk order.
+ *    several chunks leaves one partial sum per chunk in its scratch slot of
+ *    `partials` and the warp that finishes last (a ticket in the counter of
+ *    the row's first slot) adds them in chunk order.
  * All sums use compensated (Dot2) accumulation in the value's real type, so
  * results do not depend on the unit split.
  * Replaces _triton_spmv_csr_impl_prepared / _spmv_csr_real_kernel
@@ -128,7 +129,8 @@ typedef struct fsb_spmv_unit {
   int32_t tag;               /* >= 0: row block ending before row `tag`;
                                 < 0: chunk -(tag+1) of a long row                      */
   int32_t n_chunks;          /* chunks of that long row (1 for row blocks)             */
-  int32_t reserved;
+  int32_t slot;              /* scratch slot of a chunk of a row of >= 2 chunks; the
+                                row's slots are consecutive.  -1 for other units       */
 } fsb_spmv_unit;
 
 typedef struct fsb_spmv_plan {
@@ -137,10 +139,11 @@ typedef struct fsb_spmv_plan {
   const fsb_spmv_unit* units;/* [n_units]    unit descriptors                                */
   int64_t n_segs;
   int64_t n_units;
+  int64_t n_slots;           /* scratch slots, see fsb_spmv_unit.slot                        */
   int32_t cap;               /* row-block window, see above                                  */
   int32_t chunk_nnz;         /* nonzeros per long-row chunk                                  */
-  void* partials;            /* scratch: n_units * fsb_spmv_partial_bytes(dtype) bytes       */
-  int32_t* counters;         /* scratch: n_units int32, zero before the first call; every
+  void* partials;            /* scratch: n_slots * fsb_spmv_partial_bytes(dtype) bytes       */
+  int32_t* counters;         /* scratch: n_slots int32, zero before the first call; every
                                 call leaves them zero again                                  */
   int32_t flags;             /* FSB_SPMV_* bits                                              */
   int32_t reserved;
@@ -155,7 +158,7 @@ FSB_API int32_t fsb_spmv_default_cap(int dtype);
 FSB_API int32_t fsb_spmv_default_chunk(int dtype);
 FSB_API int64_t fsb_spmv_partial_bytes(int dtype);
 FSB_API int64_t fsb_spmv_plan_workspace_bytes(int64_t n_rows);
-/* d_totals (device int64[2]) receives n_segs and n_units. */
+/* d_totals (device int64[3]) receives n_segs, n_units and n_slots. */
 FSB_API int fsb_spmv_plan_analyze(const void* indptr, int ptr_is_64, int64_t n_rows, int32_t cap,
                           int32_t chunk_nnz, void* workspace, int64_t workspace_bytes,
                           int64_t* d_totals, void* stream);

@@ -212,13 +212,14 @@ void oracle_bucketize(int64_t m, const int64_t* ptr, const int64_t* ub, int nb, 
 }
 
 /* ---- SpMV unit plan (segments, units) -------------------------------- */
-/* totals[0] = segments, totals[1] = units; arrays may be NULL (count only).
- * unit descriptors (when `units` != NULL) are 5 int64 per unit:
- * nnz_begin, nnz_end, row, tag, n_chunks (tag >= 0: row block ending before
- * row `tag`; tag < 0: chunk -(tag+1) of a long row). */
+/* totals[0] = segments, totals[1] = units, totals[2] = scratch slots; arrays
+ * may be NULL (count only).  Unit descriptors (when `units` != NULL) are 6
+ * int64 per unit: nnz_begin, nnz_end, row, tag, n_chunks, slot (tag >= 0: row
+ * block ending before row `tag`; tag < 0: chunk -(tag+1) of a long row; slot
+ * numbers the chunks of rows of >= 2 chunks consecutively, -1 elsewhere). */
 void oracle_spmv_plan(int64_t m, const int64_t* ptr, int64_t cap, int64_t chunk, int64_t* totals, int32_t* seg_row0,
                       int32_t* seg_unit0, int64_t* units) {
-  int64_t s = 0, u = 0;
+  int64_t s = 0, u = 0, sl = 0;
   int64_t prev_start = -1;
   for (int64_t r = 0; r <= m; ++r) {
     int start = 0;
@@ -242,23 +243,26 @@ void oracle_spmv_plan(int64_t m, const int64_t* ptr, int64_t cap, int64_t chunk,
           int64_t nch = (len0 + chunk - 1) / chunk;
           for (int64_t k = 0; k < nch; ++k) {
             if (units) {
-              int64_t* d = units + 5 * (u + k);
+              int64_t* d = units + 6 * (u + k);
               d[0] = ptr[r0] + k * chunk;
               d[1] = ptr[r0] + ((k + 1) * chunk < len0 ? (k + 1) * chunk : len0);
               d[2] = r0;
               d[3] = -(k + 1);
               d[4] = nch;
+              d[5] = nch > 1 ? sl + k : -1;
             }
           }
           u += nch;
+          if (nch > 1) sl += nch;
         } else {
           if (units) {
-            int64_t* d = units + 5 * u;
+            int64_t* d = units + 6 * u;
             d[0] = ptr[r0];
             d[1] = ptr[r];
             d[2] = r0;
             d[3] = r;
             d[4] = 1;
+            d[5] = -1;
           }
           u += 1;
         }
@@ -275,4 +279,5 @@ void oracle_spmv_plan(int64_t m, const int64_t* ptr, int64_t cap, int64_t chunk,
   if (seg_unit0) seg_unit0[s] = (int32_t)u;
   totals[0] = s;
   totals[1] = u;
+  totals[2] = sl;
 }

@@ -182,16 +182,16 @@ def bucketize(indptr, upper_bounds):
 def spmv_plan(indptr, cap, chunk):
     """(seg_row0, seg_unit0, units) of the native SpMV unit plan.
 
-    ``units`` is int64 [n_units, 5]: nnz_begin, nnz_end, row, tag, n_chunks.
+    ``units`` is int64 [n_units, 6]: nnz_begin, nnz_end, row, tag, n_chunks, slot.
     """
     ptr = _a(indptr, np.int64)
     m = ptr.size - 1
-    totals = np.zeros(2, dtype=np.int64)
+    totals = np.zeros(3, dtype=np.int64)
     lib().oracle_spmv_plan(m, _ptr(ptr), int(cap), int(chunk), _ptr(totals), None, None, None)
     s, u = int(totals[0]), int(totals[1])
     seg_row0 = np.empty(s + 1, dtype=np.int32)
     seg_unit0 = np.empty(s + 1, dtype=np.int32)
-    units = np.empty((max(u, 1), 5), dtype=np.int64)
+    units = np.empty((max(u, 1), 6), dtype=np.int64)
     lib().oracle_spmv_plan(m, _ptr(ptr), int(cap), int(chunk), _ptr(totals), _ptr(seg_row0), _ptr(seg_unit0),
                            _ptr(units))
     return seg_row0, seg_unit0, units[:u]
