@@ -21,6 +21,7 @@ FSB_ERR_LAUNCH = -3
 FSB_ERR_TIMEOUT = -4
 FSB_ERR_CUDA = -5
 FSB_ERR_WORKSPACE = -6
+FSB_ERR_TOO_LARGE = -7
 
 DTYPE_CODE = {
     torch.float16: 0,
@@ -58,6 +59,7 @@ class SpmvPlan(ctypes.Structure):
 
 
 FSB_SPMV_FAST_SHORT_ROWS = 1
+FSB_SPMV_STATIC_MAX_SLOTS = 65536
 
 
 # name -> (restype, argtypes)
@@ -89,6 +91,11 @@ _SIGNATURES = {
         [_c_ptr, _c_int, _c_i64, _c_i32, _c_i32, _c_ptr, _c_i64, _c_ptr, _c_ptr, _c_ptr, _c_ptr],
     ),
     "fsb_spmv_csr": (
+        _c_int,
+        [_c_int, _c_ptr, _c_ptr, _c_int, _c_ptr, _c_int, _c_i64, _c_i64, _c_ptr, _c_ptr,
+         ctypes.POINTER(SpmvPlan), _c_ptr],
+    ),
+    "fsb_spmv_csr_static_scratch": (
         _c_int,
         [_c_int, _c_ptr, _c_ptr, _c_int, _c_ptr, _c_int, _c_i64, _c_i64, _c_ptr, _c_ptr,
          ctypes.POINTER(SpmvPlan), _c_ptr],

@@ -345,6 +345,7 @@ const char* fsb_status_string(int status) {
     case FSB_ERR_TIMEOUT: return "bounded device wait expired";
     case FSB_ERR_CUDA: return "CUDA runtime error";
     case FSB_ERR_WORKSPACE: return "workspace too small";
+    case FSB_ERR_TOO_LARGE: return "plan needs more scratch slots than the built-in scratch holds";
     default: return "unknown status";
   }
 }

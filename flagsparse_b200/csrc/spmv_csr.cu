@@ -20,6 +20,8 @@
 // Replaces _spmv_csr_real_kernel / _spmv_csr_complex_kernel
 // (sparse_operations/spmv_csr.py:179-240) and the bucketed CSR-vector kernels
 // (spmv_csr.py:247-368) of flagos-ai/FlagSparse.
+#include <atomic>
+#include <mutex>
 #include <type_traits>
 
 #include "fsb_common.cuh"
@@ -427,6 +429,44 @@ static int spmv_dispatch_idx(const void* data, const void* idx, int i64, const v
              : spmv_launch<DT, int32_t, int32_t>(data, idx, ptr, x, y, plan, st);
 }
 
+// ---------------------------------------------------------------------------
+// Built-in long-row scratch of fsb_spmv_csr_static_scratch: partial sums of
+// the widest type (c128, 32 bytes) for every slot, then one int32 ticket per
+// slot.  Zero at module load; every call clears the tickets it uses.
+// ---------------------------------------------------------------------------
+constexpr int64_t kStaticSlots = FSB_SPMV_STATIC_MAX_SLOTS;
+constexpr int64_t kStaticPartialBytes = 4 * sizeof(double);
+constexpr int64_t kStaticTicketOffset = kStaticSlots * kStaticPartialBytes;
+static __device__ __align__(256) unsigned char g_spmv_static_scratch[kStaticTicketOffset + kStaticSlots * sizeof(int32_t)];
+
+constexpr int kStaticMaxDevices = 256;
+static std::atomic<void*> g_static_addr[kStaticMaxDevices];
+static std::mutex g_static_mu;
+
+// Device address of the current device's scratch; resolved once per device.
+static int static_scratch_address(void** out) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return FSB_ERR_CUDA;
+  }
+  if (dev < 0 || dev >= kStaticMaxDevices) return FSB_ERR_UNSUPPORTED;
+  void* p = g_static_addr[dev].load(std::memory_order_acquire);
+  if (!p) {
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    p = g_static_addr[dev].load(std::memory_order_relaxed);
+    if (!p) {
+      if (cudaGetSymbolAddress(&p, g_spmv_static_scratch) != cudaSuccess || !p) {
+        (void)cudaGetLastError();
+        return FSB_ERR_CUDA;
+      }
+      g_static_addr[dev].store(p, std::memory_order_release);
+    }
+  }
+  *out = p;
+  return FSB_OK;
+}
+
 }  // namespace fsb
 
 using namespace fsb;
@@ -461,6 +501,31 @@ int fsb_spmv_csr(int dtype, const void* data, const void* indices, int idx_is_64
     case FSB_C128: return spmv_dispatch_idx<FSB_C128>(data, indices, idx_is_64, indptr, ptr_is_64, x, y, *plan, st);
     default: return FSB_ERR_UNSUPPORTED;
   }
+}
+
+int fsb_spmv_csr_static_scratch(int dtype, const void* data, const void* indices, int idx_is_64, const void* indptr,
+                                int ptr_is_64, int64_t n_rows, int64_t n_cols, const void* x, void* y,
+                                const fsb_spmv_plan* plan, void* stream) {
+  if (!plan || n_rows < 0 || n_cols < 0 || plan->n_slots < 0) return FSB_ERR_INVALID_ARG;
+  if (plan->n_slots > kStaticSlots) return FSB_ERR_TOO_LARGE;
+  if (fsb_spmv_partial_bytes(dtype) < 0) return FSB_ERR_UNSUPPORTED;
+  if (n_rows == 0 || plan->n_units == 0) return FSB_OK;
+  fsb_spmv_plan p = *plan;
+  p.partials = nullptr;
+  p.counters = nullptr;
+  if (p.n_slots > 0) {
+    void* base = nullptr;
+    const int rc = static_scratch_address(&base);
+    if (rc != FSB_OK) return rc;
+    p.partials = base;
+    p.counters = reinterpret_cast<int32_t*>(static_cast<unsigned char*>(base) + kStaticTicketOffset);
+    if (cudaMemsetAsync(p.counters, 0, size_t(p.n_slots) * sizeof(int32_t), static_cast<cudaStream_t>(stream)) !=
+        cudaSuccess) {
+      (void)cudaGetLastError();
+      return FSB_ERR_CUDA;
+    }
+  }
+  return fsb_spmv_csr(dtype, data, indices, idx_is_64, indptr, ptr_is_64, n_rows, n_cols, x, y, &p, stream);
 }
 
 }  // extern "C"

@@ -34,6 +34,7 @@ extern "C" {
 #define FSB_ERR_TIMEOUT (-4)       /* a bounded device wait gave up             */
 #define FSB_ERR_CUDA (-5)          /* other CUDA runtime error                  */
 #define FSB_ERR_WORKSPACE (-6)     /* caller workspace too small                */
+#define FSB_ERR_TOO_LARGE (-7)     /* plan exceeds a fixed built-in scratch     */
 
 /* ---- value dtype codes (torch dtype -> code mapping lives in _native.py) -- */
 #define FSB_F16 0
@@ -169,6 +170,42 @@ FSB_API int fsb_spmv_plan_build(const void* indptr, int ptr_is_64, int64_t n_row
 FSB_API int fsb_spmv_csr(int dtype, const void* data, const void* indices, int idx_is_64,
                  const void* indptr, int ptr_is_64, int64_t n_rows, int64_t n_cols,
                  const void* x, void* y, const fsb_spmv_plan* plan, void* stream);
+
+/* ------------------------------------------------------------------------
+ * CSR SpMV with built-in scratch: allocates nothing on any call.
+ *
+ * No counterpart in flagos-ai/FlagSparse, whose SpMV allocates its output and
+ * temporaries with torch on every call.  This entry point serves callers that
+ * must not allocate device memory on the call path: code running where an
+ * allocation could block or fail at the wrong time (a real-time loop with a
+ * fixed memory budget, a caller that owns no allocator, a stream about to be
+ * captured).
+ *
+ * Same arguments and results as fsb_spmv_csr (bit-identical output), except
+ * that plan->partials and plan->counters are ignored (they may be NULL): the
+ * long-row scratch is one file-scope device array of this library,
+ * FSB_SPMV_STATIC_MAX_SLOTS slots (32 bytes of partial sum + one int32 ticket
+ * each, 2.25 MiB per device).  A plan with n_slots > FSB_SPMV_STATIC_MAX_SLOTS
+ * is rejected with FSB_ERR_TOO_LARGE before any work is enqueued; use
+ * fsb_spmv_csr with caller scratch for it.  65536 slots cover every plan whose
+ * multi-chunk long rows hold at most 65536 * chunk_nnz nonzeros (33.5 M at the
+ * default chunk).
+ *
+ * The scratch is the current device's: `stream` must belong to the device
+ * current on the calling thread.  The first call on a device resolves the
+ * scratch address with cudaGetSymbolAddress (once per device, device current,
+ * status checked; failure returns FSB_ERR_CUDA); make that first call before
+ * any stream capture begins.  Every call clears the n_slots tickets the plan
+ * uses (cudaMemsetAsync on `stream`) before its kernel.
+ *
+ * One scratch per device: calls whose kernels can overlap on the GPU (other
+ * streams, other threads, other plans) race on it and give wrong results.
+ * Serialise them, e.g. by issuing all such calls on one stream.
+ * ------------------------------------------------------------------------ */
+#define FSB_SPMV_STATIC_MAX_SLOTS 65536
+FSB_API int fsb_spmv_csr_static_scratch(int dtype, const void* data, const void* indices, int idx_is_64,
+                                const void* indptr, int ptr_is_64, int64_t n_rows, int64_t n_cols,
+                                const void* x, void* y, const fsb_spmv_plan* plan, void* stream);
 
 #ifdef __cplusplus
 }  /* extern "C" */
