@@ -23,7 +23,6 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -57,62 +56,83 @@ def _ncu_traffic(workload):
 
 
 class ClockSampler:
-    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+    """Polls SM clocks and clock-event reasons through NVML (read-only) every ~1 ms.
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    Samples carry host timestamps; ``mark`` records the bounds of the timed
+    region, and ``stop`` summarises the samples taken inside it (widened to
+    the whole measured phase when the timed region is too short to hold a
+    few samples).  Reports None when NVML is unusable.
+    """
 
-    def __init__(self, gpu_index):
-        self.gpu = str(gpu_index)
-        self.proc = None
-        self.lines = []
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
+
+    def __init__(self, cuda_index):
+        self.cuda_index = int(cuda_index)
+        self.samples = []  # (t, sm_mhz, max_mhz, reasons bitmask)
+        self.marks = {}
+        self._stop = threading.Event()
         self.thread = None
+        self.source = None
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
-                 "-i", self.gpu],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except (OSError, FileNotFoundError):
-            self.proc = None
-            return
-        self.thread = threading.Thread(target=self._read, daemon=True)
-        self.thread.start()
+            import pynvml
+            import torch
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            pynvml.nvmlInit()
+            idx = torch.cuda._get_nvml_device_index(self.cuda_index)
+            self._nvml = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(idx)
+            self._max = float(pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM))
+            self._bits = {name: getattr(pynvml, attr, 0) for name, attr in self.REASONS}
+            self.source = "nvml"
+        except Exception:
+            self.source = None
+            return
+        self.thread = threading.Thread(target=self._poll, daemon=True)
+        self.thread.start()
+        t0 = time.monotonic()
+        while not self.samples and time.monotonic() - t0 < 2.0:
+            time.sleep(0.001)
+
+    def _poll(self):
+        nv, h = self._nvml, self._h
+        while not self._stop.is_set():
+            try:
+                sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))
+            except Exception:
+                break
+            self.samples.append((time.monotonic(), sm, self._max, rs))
+            time.sleep(0.001)
+
+    def mark(self, name):
+        self.marks[name] = time.monotonic()
 
     def stop(self):
-        if self.proc is None:
+        if self.thread is None:
             return None
-        self.proc.terminate()
+        self._stop.set()
+        self.thread.join(timeout=2)
         try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        if self.thread:
-            self.thread.join(timeout=2)
-        sm, smax, reasons = [], [], set()
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for line in self.lines:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
-            except ValueError:
-                continue
-            for name, val in zip(names, parts[5:9]):
-                if val.lower() == "active":
-                    reasons.add(name)
-        if not sm:
+            self._nvml.nvmlShutdown()
+        except Exception:
+            pass
+        t0, t1 = self.marks.get("timed_start", 0.0), self.marks.get("timed_end", float("inf"))
+        window = "timed"
+        sel = [s for s in self.samples if t0 <= s[0] <= t1]
+        if len(sel) < 3:
+            t1 = self.marks.get("phase_end", t1)
+            sel = [s for s in self.samples if t0 <= s[0] <= t1]
+            window = "timed+e2e (timed region shorter than the poll interval)"
+        if not sel:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        reasons = sorted(name for name, bit in self._bits.items() if bit and any(s[3] & bit for s in sel))
+        return {"sm_mhz": statistics.median(s[1] for s in sel), "sm_max_mhz": max(s[2] for s in sel),
+                "reasons": reasons, "samples": len(sel), "window": window, "source": self.source}
 
 
 # ---------------------------------------------------------------- workloads
@@ -231,12 +251,14 @@ def main():
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     barrier()
     torch.cuda.synchronize()
+    sampler.mark("timed_start")
     for i in range(args.steps):
         flush.fill_(float(i))
         starts[i].record()
         wl.step()
         ends[i].record()
     torch.cuda.synchronize()
+    sampler.mark("timed_end")
     barrier()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     t_ms = sum(step_ms)
@@ -254,6 +276,7 @@ def main():
         wl.e2e_step()
     e1.record()
     torch.cuda.synchronize()
+    sampler.mark("phase_end")
     barrier()
     clocks = sampler.stop()
     e2e_ms = e0.elapsed_time(e1)

@@ -10,8 +10,36 @@ __version__ = "1.0.0"
 
 _OPS_EXPORTS = {
     "PreparedCsrSpmv",
+    "PreparedCsrSpmmOpt",
+    "PreparedCsrSpmmOptAlg2",
+    "PreparedCsrSpmmRoute",
+    "SDDMMPrepared",
+    "SpmmCsrAlgorithm",
+    "SpmmCsrAlgorithmUnavailable",
     "prepare_spmv_csr",
+    "prepare_spmm_csr_route",
+    "prepare_spmm_csr_opt",
+    "prepare_spmm_csr_opt_alg1",
+    "prepare_spmm_csr_opt_alg1_preprocess",
+    "prepare_spmm_csr_opt_alg2",
+    "prepare_spmm_csr_opt_alg2_preprocess",
+    "prepare_sddmm_csr",
     "flagsparse_spmv_csr",
+    "flagsparse_spmm_csr",
+    "flagsparse_spmm_csr_run",
+    "flagsparse_spmm_csr_opt",
+    "flagsparse_spmm_csr_opt_alg1",
+    "flagsparse_spmm_csr_opt_alg1_preprocess",
+    "flagsparse_spmm_csr_opt_alg2",
+    "flagsparse_spmm_csr_opt_alg2_preprocess",
+    "flagsparse_sddmm_csr",
+    "list_spmm_csr_algorithms",
+    "resolve_spmm_csr_algorithm",
+    # differentiable SpMM (no FlagSparse counterpart)
+    "CsrSpmmFunction",
+    "PreparedCsrSpmmAutograd",
+    "prepare_spmm_csr_autograd",
+    "flagsparse_spmm_csr_autograd",
 }
 
 __all__ = sorted(_OPS_EXPORTS)

@@ -60,6 +60,9 @@ class SpmvPlan(ctypes.Structure):
 
 FSB_SPMV_FAST_SHORT_ROWS = 1
 FSB_SPMV_STATIC_MAX_SLOTS = 65536
+FSB_SPMM_COMPENSATED = 2
+FSB_SDDMM_ACC64 = 1
+FSB_SDDMM_OUT64 = 2
 
 
 # name -> (restype, argtypes)
@@ -94,6 +97,20 @@ _SIGNATURES = {
         _c_int,
         [_c_int, _c_ptr, _c_ptr, _c_int, _c_ptr, _c_int, _c_i64, _c_i64, _c_ptr, _c_ptr,
          ctypes.POINTER(SpmvPlan), _c_ptr],
+    ),
+    "fsb_spmm_default_cap": (_c_i32, [_c_int]),
+    "fsb_spmm_default_chunk": (_c_i32, [_c_int]),
+    "fsb_spmm_scratch_layout": (_c_int, [_c_int, _c_i64, _c_i64p, _c_i64p]),
+    "fsb_spmm_csr": (
+        _c_int,
+        [_c_int, _c_ptr, _c_ptr, _c_ptr, _c_i64, _c_i64, _c_ptr, _c_i64, _c_i64, _c_ptr, _c_i64,
+         ctypes.POINTER(SpmvPlan), _c_ptr],
+    ),
+    "fsb_csr_row_ids": (_c_int, [_c_ptr, _c_int, _c_i64, _c_i64, _c_ptr, _c_ptr]),
+    "fsb_sddmm_csr": (
+        _c_int,
+        [_c_int, _c_ptr, _c_ptr, _c_i64, _c_ptr, _c_i64, _c_ptr, _c_i64, _c_i64, _c_ptr,
+         ctypes.c_double, ctypes.c_double, _c_ptr, _c_int, _c_ptr],
     ),
     "fsb_spmv_csr_static_scratch": (
         _c_int,

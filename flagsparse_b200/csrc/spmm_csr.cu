@@ -1,0 +1,435 @@
+// CSR SpMM  C = A B  for sm_100a (A sparse M x K in CSR, B dense K x N row-major).
+//
+// The launch reuses the SpMV unit plan (plan.cu), built with the SpMM window
+// cap (64) and chunk (256): every warp executes one (unit, column tile) pair.
+// The lanes of a warp own consecutive column groups of V elements of the tile
+// (16-byte loads when N and the leading dimensions allow it), so one nonzero
+// costs the warp a single coalesced read of its B-row slice:
+//
+//  * row-block unit: a run of rows with < 128 nonzeros.  The warp stages the
+//    nonzeros (value, column, local row) in its shared-memory slice, writes
+//    zero rows for empty rows, then walks the nonzeros in order, loading the
+//    B slices of 4 nonzeros ahead of the multiply-adds across row boundaries
+//    and storing a C row slice whenever the row changes.
+//  * long-row chunk: `chunk_nnz` nonzeros of a row with > cap nonzeros, staged
+//    in 128-nonzero batches.  A one-chunk row is written directly; otherwise
+//    the chunk's partial row slice goes to its scratch slot and the warp that
+//    completes the row's ticket adds the partials in chunk order.
+//
+// Accumulation: fp32 for half / bfloat16 / fp32 values (half and bfloat16
+// products are exact in fp32), fp64 for fp64, componentwise for complex.
+// FSB_SPMM_COMPENSATED switches every sum to Dot2 compensated accumulation.
+// Every sum runs in a fixed order, so results are bitwise reproducible.
+//
+// Replaces _triton_spmm_csr_impl / _spmm_csr_real_kernel / the complex kernel
+// (sparse_operations/spmm_csr.py:3373-3466, 144-339) and the bucketed
+// alg1 / alg2 / opt kernels (spmm_csr.py:1091-2449, spmm_csr_opt_alg2.py) of
+// flagos-ai/FlagSparse.
+#include <cstring>
+#include <type_traits>
+
+#include "fsb_common.cuh"
+
+namespace fsb {
+namespace {
+
+constexpr int kSpmmWarps = 8;      // warps per block; one (unit, tile) per warp
+constexpr int kSpmmBatch = 128;    // nonzeros staged per batch
+constexpr int kSpmmMaxCap = 64;    // row blocks hold < 2*cap <= kSpmmBatch nonzeros
+constexpr int kSpmmAhead = 4;      // B slices loaded ahead of the multiply-adds
+constexpr int kSpmmTileLanes = 32;
+
+template <int BYTES> struct RawT;
+template <> struct RawT<2> { using T = unsigned short; };
+template <> struct RawT<4> { using T = unsigned int; };
+template <> struct RawT<8> { using T = uint2; };
+template <> struct RawT<16> { using T = uint4; };
+
+// V consecutive elements starting at p; the first nv < V only when the slice
+// crosses column N (the rest read as zero).
+template <typename S, int V>
+__device__ __forceinline__ void load_slice(const S* p, int nv, S (&out)[V]) {
+  if (nv == V) {
+    using Raw = typename RawT<int(sizeof(S)) * V>::T;
+    Raw r = __ldg(reinterpret_cast<const Raw*>(p));
+    memcpy(out, &r, sizeof(Raw));
+  } else {
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      if (j < nv) {
+        out[j] = p[j];
+      } else {
+        memset(&out[j], 0, sizeof(S));
+      }
+    }
+  }
+}
+
+template <typename S, int V>
+__device__ __forceinline__ void store_slice(S* p, int nv, const S (&v)[V]) {
+  if (nv == V) {
+    using Raw = typename RawT<int(sizeof(S)) * V>::T;
+    Raw r;
+    memcpy(&r, v, sizeof(Raw));
+    *reinterpret_cast<Raw*>(p) = r;
+  } else {
+#pragma unroll
+    for (int j = 0; j < V; ++j)
+      if (j < nv) p[j] = v[j];
+  }
+}
+
+__device__ __forceinline__ __half spmm_store(float v, __half*) { return __float2half_rn(v); }
+__device__ __forceinline__ __nv_bfloat16 spmm_store(float v, __nv_bfloat16*) { return __float2bfloat16_rn(v); }
+__device__ __forceinline__ float spmm_store(float v, float*) { return v; }
+__device__ __forceinline__ double spmm_store(double v, double*) { return v; }
+
+// Per-lane accumulator of V output elements.
+template <int DT, bool COMP, int V>
+struct SpmmAcc {
+  using Vt = VT<DT>;
+  using S = typename Vt::Store;
+  using R = typename Vt::Real;
+  static constexpr bool kCplx = Vt::kComplex;
+  static constexpr int kNC = kCplx ? 2 : 1;            // real components per element
+  using Sum = typename std::conditional<COMP, Comp<R>, Plain<R>>::type;
+  Sum s[kNC][V];
+
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int c = 0; c < kNC; ++c)
+#pragma unroll
+      for (int j = 0; j < V; ++j) s[c][j].zero();
+  }
+
+  __device__ __forceinline__ static void term(Sum& acc, R a, R b) {
+    if constexpr (COMP && Vt::kExactProduct) acc.add(mul_rn(a, b));  // exact product
+    else acc.add_prod(a, b);
+  }
+
+  __device__ __forceinline__ void add(S a, const S (&b)[V]) {
+    if constexpr (kCplx) {
+#pragma unroll
+      for (int j = 0; j < V; ++j) {
+        term(s[0][j], a.x, b[j].x);
+        term(s[0][j], -a.y, b[j].y);
+        term(s[1][j], a.x, b[j].y);
+        term(s[1][j], a.y, b[j].x);
+      }
+    } else {
+      const R ar = to_real(a);
+#pragma unroll
+      for (int j = 0; j < V; ++j) term(s[0][j], ar, to_real(b[j]));
+    }
+  }
+
+  __device__ __forceinline__ void result(S (&out)[V]) const {
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      if constexpr (kCplx) {
+        out[j].x = s[0][j].value();
+        out[j].y = s[1][j].value();
+      } else {
+        out[j] = spmm_store(s[0][j].value(), static_cast<S*>(nullptr));
+      }
+    }
+  }
+
+  // scratch layout per element: (hi, lo) per real component
+  __device__ __forceinline__ void store_partial(R* p) const {
+#pragma unroll
+    for (int j = 0; j < V; ++j)
+#pragma unroll
+      for (int c = 0; c < kNC; ++c) {
+        p[(j * kNC + c) * 2] = s[c][j].hi;
+        if constexpr (COMP) p[(j * kNC + c) * 2 + 1] = s[c][j].lo;
+        else p[(j * kNC + c) * 2 + 1] = R(0);
+      }
+  }
+
+  __device__ __forceinline__ void add_partial(const R* p) {
+#pragma unroll
+    for (int j = 0; j < V; ++j)
+#pragma unroll
+      for (int c = 0; c < kNC; ++c)
+        s[c][j].add_comp(__ldcg(p + (j * kNC + c) * 2), __ldcg(p + (j * kNC + c) * 2 + 1));
+  }
+};
+
+// Per-warp shared-memory slice: staged values, columns, the unit's row
+// offsets and each staged nonzero's local row; a multiple of 16 bytes.
+template <typename S>
+constexpr int spmm_warp_smem_bytes() {
+  return (kSpmmBatch * int(sizeof(S)) + kSpmmBatch * 4 + (kSpmmMaxCap + 1) * 4 + kSpmmBatch + 15) & ~15;
+}
+
+template <int DT>
+struct SpmmMinBlocks { static constexpr int value = (DT == FSB_C128) ? 2 : (DT == FSB_F64 || DT == FSB_C64) ? 3 : 4; };
+
+template <typename T> __device__ __forceinline__ T ld_once(const T* p) { return __ldcs(p); }
+template <> __device__ __forceinline__ __half ld_once<__half>(const __half* p) {
+  return __ushort_as_half(__ldcs(reinterpret_cast<const unsigned short*>(p)));
+}
+template <> __device__ __forceinline__ __nv_bfloat16 ld_once<__nv_bfloat16>(const __nv_bfloat16* p) {
+  return __ushort_as_bfloat16(__ldcs(reinterpret_cast<const unsigned short*>(p)));
+}
+
+// grid: x = groups of kSpmmWarps units, y = column tiles of 32*V columns.
+// pstride: scratch elements per slot; cps: tickets per slot.
+template <int DT, int V, bool COMP>
+__global__ void __launch_bounds__(kSpmmWarps * 32, SpmmMinBlocks<DT>::value)
+k_spmm_csr(const typename VT<DT>::Store* __restrict__ data, const int32_t* __restrict__ col,
+           const int64_t* __restrict__ ptr, const typename VT<DT>::Store* __restrict__ B, int64_t ldb, int64_t n,
+           typename VT<DT>::Store* __restrict__ C, int64_t ldc, fsb_spmv_plan plan, int64_t pstride, int64_t cps) {
+  using S = typename VT<DT>::Store;
+  using R = typename VT<DT>::Real;
+  using Acc = SpmmAcc<DT, COMP, V>;
+  constexpr int kER = Acc::kNC * 2;  // scratch reals per element
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t unit = int64_t(blockIdx.x) * kSpmmWarps + warp;
+  if (unit >= plan.n_units) return;  // whole warp leaves together
+  const int tile = blockIdx.y;
+  const int64_t c0 = int64_t(tile) * (kSpmmTileLanes * V) + int64_t(lane) * V;  // this lane's first column
+  const int nv = static_cast<int>(n - c0 >= V ? int64_t(V) : (n > c0 ? n - c0 : int64_t(0)));
+
+  unsigned char* wbase = smem_raw + warp * spmm_warp_smem_bytes<S>();
+  S* sh_a = reinterpret_cast<S*>(wbase);
+  int32_t* sh_c = reinterpret_cast<int32_t*>(wbase + kSpmmBatch * sizeof(S));
+  int32_t* sh_off = sh_c + kSpmmBatch;
+  uint8_t* sh_rid = reinterpret_cast<uint8_t*>(sh_off + kSpmmMaxCap + 1);
+
+  const fsb_spmv_unit* ud = plan.units + unit;
+  const int64_t s0 = __ldg(&ud->nnz_begin), s1 = __ldg(&ud->nnz_end);
+  const int32_t row = __ldg(&ud->row), tag = __ldg(&ud->tag);
+
+  auto flush = [&](const Acc& acc, int64_t r) {
+    if (nv > 0) {
+      S o[V];
+      acc.result(o);
+      store_slice(C + r * ldc + c0, nv, o);
+    }
+  };
+
+  if (tag >= 0) {
+    // ------------------------------------------------------------ row block
+    const int nr = tag - row;
+    const int cnt = static_cast<int>(s1 - s0);
+    for (int i = lane; i <= nr; i += 32) sh_off[i] = static_cast<int32_t>(__ldg(ptr + row + i) - s0);
+    for (int k = lane; k < cnt; k += 32) {
+      sh_a[k] = ld_once(data + s0 + k);
+      sh_c[k] = ld_once(col + s0 + k);
+    }
+    __syncwarp();
+    for (int k = lane; k < cnt; k += 32) {  // local row of nonzero k: first i with off[i+1] > k
+      int lo = 0, hi = nr - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (sh_off[mid + 1] > k) hi = mid; else lo = mid + 1;
+      }
+      sh_rid[k] = static_cast<uint8_t>(lo);
+    }
+    for (int i0 = 0; i0 < nr; i0 += 32) {  // empty rows get zero slices
+      const int i = i0 + lane;
+      unsigned m = __ballot_sync(0xffffffffu, i < nr && sh_off[i] == sh_off[i + 1]);
+      while (m) {
+        const int b = __ffs(m) - 1;
+        m &= m - 1;
+        Acc z;
+        z.zero();
+        flush(z, int64_t(row) + i0 + b);
+      }
+    }
+    __syncwarp();
+    if (cnt == 0) return;
+    Acc acc;
+    acc.zero();
+    int cur = sh_rid[0];
+    for (int k = 0; k < cnt; k += kSpmmAhead) {
+      S bv[kSpmmAhead][V];
+#pragma unroll
+      for (int u = 0; u < kSpmmAhead; ++u) {
+        const int kk = k + u < cnt ? k + u : k;
+        load_slice<S, V>(B + int64_t(sh_c[kk]) * ldb + c0, k + u < cnt ? nv : 0, bv[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < kSpmmAhead; ++u) {
+        if (k + u < cnt) {
+          const int r = sh_rid[k + u];
+          if (r != cur) {  // uniform across the warp
+            flush(acc, int64_t(row) + cur);
+            acc.zero();
+            cur = r;
+          }
+          acc.add(sh_a[k + u], bv[u]);
+        }
+      }
+    }
+    flush(acc, int64_t(row) + cur);
+    return;
+  }
+
+  // ------------------------------------------------------------ long-row chunk
+  const int32_t nch = __ldg(&ud->n_chunks), slot = __ldg(&ud->slot);
+  Acc acc;
+  acc.zero();
+  for (int64_t b0 = s0; b0 < s1; b0 += kSpmmBatch) {
+    const int cnt = static_cast<int>(s1 - b0 < kSpmmBatch ? s1 - b0 : int64_t(kSpmmBatch));
+    __syncwarp();
+    for (int k = lane; k < cnt; k += 32) {
+      sh_a[k] = ld_once(data + b0 + k);
+      sh_c[k] = ld_once(col + b0 + k);
+    }
+    __syncwarp();
+    for (int k = 0; k < cnt; k += kSpmmAhead) {
+      S bv[kSpmmAhead][V];
+#pragma unroll
+      for (int u = 0; u < kSpmmAhead; ++u) {
+        const int kk = k + u < cnt ? k + u : k;
+        load_slice<S, V>(B + int64_t(sh_c[kk]) * ldb + c0, k + u < cnt ? nv : 0, bv[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < kSpmmAhead; ++u)
+        if (k + u < cnt) acc.add(sh_a[k + u], bv[u]);
+    }
+  }
+  if (nch == 1) {
+    flush(acc, row);
+    return;
+  }
+  R* part = static_cast<R*>(plan.partials);
+  const int64_t first = int64_t(slot) + (tag + 1);  // slot of the row's first chunk
+  acc.store_partial(part + (int64_t(slot) * pstride + c0) * kER);
+  __threadfence();
+  __syncwarp();
+  int ticket = 0;
+  if (lane == 0) ticket = atomicAdd(plan.counters + first * cps + tile, 1);
+  ticket = __shfl_sync(0xffffffffu, ticket, 0);
+  if (ticket != nch - 1) return;
+  __threadfence();
+  Acc fin;
+  fin.zero();
+#pragma unroll 4
+  for (int c = 0; c < nch; ++c) fin.add_partial(part + ((first + c) * pstride + c0) * kER);
+  flush(fin, row);
+  if (lane == 0) plan.counters[first * cps + tile] = 0;  // ready for the next call
+}
+
+}  // namespace
+}  // namespace fsb
+
+namespace fsb {
+namespace {
+
+inline int64_t spmm_real_bytes(int dtype) {
+  switch (dtype) {
+    case FSB_F16: case FSB_BF16: case FSB_F32: case FSB_C64: return 4;
+    case FSB_F64: case FSB_C128: return 8;
+    default: return -1;
+  }
+}
+
+inline int64_t spmm_pstride(int64_t n) { return ceil_div(n, 256) * 256; }
+inline int64_t spmm_cps(int64_t n) { return n > 32 ? ceil_div(n, 32) : 1; }
+
+template <int DT, int V, bool COMP>
+int spmm_launch_v(const void* data, const int32_t* idx, const int64_t* ptr, const void* B, int64_t ldb, int64_t n,
+                  void* C, int64_t ldc, const fsb_spmv_plan& plan, cudaStream_t st) {
+  using S = typename VT<DT>::Store;
+  const int64_t tiles = ceil_div(n, kSpmmTileLanes * V);
+  if (tiles > 65535) return FSB_ERR_UNSUPPORTED;
+  const int64_t blocks = ceil_div(plan.n_units, kSpmmWarps);
+  const size_t smem = size_t(spmm_warp_smem_bytes<S>()) * kSpmmWarps;
+  dim3 grid((unsigned)blocks, (unsigned)tiles);
+  k_spmm_csr<DT, V, COMP><<<grid, kSpmmWarps * 32, smem, st>>>(
+      static_cast<const S*>(data), idx, ptr, static_cast<const S*>(B), ldb, n, static_cast<S*>(C), ldc, plan,
+      spmm_pstride(n), spmm_cps(n));
+  FSB_LAUNCH_CHECK();
+  return FSB_OK;
+}
+
+// Widest per-lane vector (elements) that 32 lanes need for N columns and that
+// the B / C base addresses and leading dimensions allow.
+template <int DT>
+int spmm_pick_v(const void* B, int64_t ldb, const void* C, int64_t ldc, int64_t n) {
+  using S = typename VT<DT>::Store;
+  constexpr int kVmax = 16 / int(sizeof(S));
+  int v = 1;
+  while (v < kVmax && int64_t(kSpmmTileLanes) * v < n) v *= 2;
+  auto ok = [&](int w) {
+    const uintptr_t a = uintptr_t(w) * sizeof(S);
+    return reinterpret_cast<uintptr_t>(B) % a == 0 && reinterpret_cast<uintptr_t>(C) % a == 0 && ldb % w == 0 &&
+           ldc % w == 0;
+  };
+  while (v > 1 && !ok(v)) v /= 2;
+  return v;
+}
+
+template <int DT, bool COMP>
+int spmm_dispatch(const void* data, const int32_t* idx, const int64_t* ptr, const void* B, int64_t ldb, int64_t n,
+                  void* C, int64_t ldc, const fsb_spmv_plan& plan, cudaStream_t st) {
+  using S = typename VT<DT>::Store;
+  constexpr int kVmax = 16 / int(sizeof(S));
+  const int v = spmm_pick_v<DT>(B, ldb, C, ldc, n);
+  if constexpr (kVmax >= 8)
+    if (v == 8) return spmm_launch_v<DT, 8, COMP>(data, idx, ptr, B, ldb, n, C, ldc, plan, st);
+  if constexpr (kVmax >= 4)
+    if (v == 4) return spmm_launch_v<DT, 4, COMP>(data, idx, ptr, B, ldb, n, C, ldc, plan, st);
+  if constexpr (kVmax >= 2)
+    if (v == 2) return spmm_launch_v<DT, 2, COMP>(data, idx, ptr, B, ldb, n, C, ldc, plan, st);
+  return spmm_launch_v<DT, 1, COMP>(data, idx, ptr, B, ldb, n, C, ldc, plan, st);
+}
+
+template <int DT>
+int spmm_mode(const void* data, const int32_t* idx, const int64_t* ptr, const void* B, int64_t ldb, int64_t n,
+              void* C, int64_t ldc, const fsb_spmv_plan& plan, cudaStream_t st) {
+  if (plan.flags & FSB_SPMM_COMPENSATED) return spmm_dispatch<DT, true>(data, idx, ptr, B, ldb, n, C, ldc, plan, st);
+  return spmm_dispatch<DT, false>(data, idx, ptr, B, ldb, n, C, ldc, plan, st);
+}
+
+}  // namespace
+}  // namespace fsb
+
+using namespace fsb;
+
+extern "C" {
+
+int32_t fsb_spmm_default_cap(int dtype) { (void)dtype; return kSpmmMaxCap; }
+
+int32_t fsb_spmm_default_chunk(int dtype) { (void)dtype; return 2 * kSpmmBatch; }
+
+int fsb_spmm_scratch_layout(int dtype, int64_t n, int64_t* partial_bytes_per_slot, int64_t* tickets_per_slot) {
+  const int64_t rb = spmm_real_bytes(dtype);
+  if (rb < 0) return FSB_ERR_UNSUPPORTED;
+  if (n < 0 || !partial_bytes_per_slot || !tickets_per_slot) return FSB_ERR_INVALID_ARG;
+  const int64_t comps = (dtype == FSB_C64 || dtype == FSB_C128) ? 2 : 1;
+  *partial_bytes_per_slot = spmm_pstride(n) * comps * 2 * rb;
+  *tickets_per_slot = spmm_cps(n);
+  return FSB_OK;
+}
+
+int fsb_spmm_csr(int dtype, const void* data, const int32_t* indices, const int64_t* indptr, int64_t n_rows,
+                 int64_t n_cols, const void* B, int64_t ldb, int64_t n, void* C, int64_t ldc,
+                 const fsb_spmv_plan* plan, void* stream) {
+  if (!plan || n_rows < 0 || n_cols < 0 || n < 0 || ldb < n || ldc < n) return FSB_ERR_INVALID_ARG;
+  if (n_rows == 0 || n == 0) return FSB_OK;
+  if (!indptr || !C || !plan->units || plan->n_units < 1 || plan->cap < 1 || plan->cap > kSpmmMaxCap ||
+      plan->chunk_nnz < kSpmmBatch || plan->chunk_nnz % kSpmmBatch != 0 || plan->n_slots < 0 ||
+      (plan->n_slots > 0 && (!plan->partials || !plan->counters)))
+    return FSB_ERR_INVALID_ARG;
+  if (n_cols > 0 && !B) return FSB_ERR_INVALID_ARG;
+  if (plan->n_units >= INT32_MAX) return FSB_ERR_UNSUPPORTED;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  switch (dtype) {
+    case FSB_F16: return spmm_mode<FSB_F16>(data, indices, indptr, B, ldb, n, C, ldc, *plan, st);
+    case FSB_BF16: return spmm_mode<FSB_BF16>(data, indices, indptr, B, ldb, n, C, ldc, *plan, st);
+    case FSB_F32: return spmm_mode<FSB_F32>(data, indices, indptr, B, ldb, n, C, ldc, *plan, st);
+    case FSB_F64: return spmm_mode<FSB_F64>(data, indices, indptr, B, ldb, n, C, ldc, *plan, st);
+    case FSB_C64: return spmm_mode<FSB_C64>(data, indices, indptr, B, ldb, n, C, ldc, *plan, st);
+    case FSB_C128: return spmm_mode<FSB_C128>(data, indices, indptr, B, ldb, n, C, ldc, *plan, st);
+    default: return FSB_ERR_UNSUPPORTED;
+  }
+}
+
+}  // extern "C"

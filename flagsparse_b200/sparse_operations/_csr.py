@@ -122,7 +122,7 @@ class NativeSpmvPlan:
     __slots__ = ("seg_row0", "seg_unit0", "units", "partials", "counters", "cap", "chunk_nnz",
                  "n_segs", "n_units", "n_slots", "dtype", "flags", "_struct")
 
-    def __init__(self, indptr, n_rows, dtype, cap=None, chunk_nnz=None, fast_short_rows=False):
+    def __init__(self, indptr, n_rows, dtype, cap=None, chunk_nnz=None, fast_short_rows=False, scratch=True):
         lib = nat.lib()
         code = nat.dtype_code(dtype)
         device = indptr.device
@@ -152,9 +152,13 @@ class NativeSpmvPlan:
                                         nat.ptr(self.seg_unit0), nat.ptr(self.units), st),
                 "fsb_spmv_plan_build",
             )
-        pbytes = int(lib.fsb_spmv_partial_bytes(code))
-        self.partials = torch.empty(max(self.n_slots * pbytes, 16), dtype=torch.uint8, device=device)
-        self.counters = torch.zeros(max(self.n_slots, 1), dtype=torch.int32, device=device)
+        if scratch:
+            pbytes = int(lib.fsb_spmv_partial_bytes(code))
+            self.partials = torch.empty(max(self.n_slots * pbytes, 16), dtype=torch.uint8, device=device)
+            self.counters = torch.zeros(max(self.n_slots, 1), dtype=torch.int32, device=device)
+        else:  # the caller attaches scratch (see SpmmPlan)
+            self.partials = None
+            self.counters = None
         self.flags = nat.FSB_SPMV_FAST_SHORT_ROWS if fast_short_rows else 0
         self._struct = nat.SpmvPlan(
             nat.ptr(self.seg_row0), nat.ptr(self.seg_unit0), nat.ptr(self.units),
@@ -179,3 +183,69 @@ class NativeSpmvPlan:
         nch = (u[:, 3] & 0xFFFFFFFF).to(torch.int64)
         slot = u[:, 3] >> 32
         return u[:, 0].numpy(), u[:, 1].numpy(), row.numpy(), tag.numpy(), nch.numpy(), slot.numpy()
+
+
+class SpmmPlan:
+    """The SpMM launch plan: a unit plan built with the SpMM window and chunk,
+    plus long-row scratch sized per dense width N (allocated once per N and
+    reused; fsb_spmm_csr leaves the tickets zero after every call)."""
+
+    def __init__(self, indptr, n_rows, dtype):
+        lib = nat.lib()
+        code = nat.dtype_code(dtype)
+        self.dtype = dtype
+        self.plan = NativeSpmvPlan(indptr, n_rows, dtype, cap=int(lib.fsb_spmm_default_cap(code)),
+                                   chunk_nnz=int(lib.fsb_spmm_default_chunk(code)), scratch=False)
+        self._scratch = {}  # n -> (partials, counters, SpmvPlan struct)
+
+    @property
+    def n_units(self):
+        return self.plan.n_units
+
+    @property
+    def n_slots(self):
+        return self.plan.n_slots
+
+    def struct_for(self, n, compensated=False):
+        """ctypes reference to an fsb_spmv_plan with scratch for dense width ``n``."""
+        key = int(n)
+        entry = self._scratch.get(key)
+        if entry is None:
+            pb, tk = ctypes.c_int64(0), ctypes.c_int64(0)
+            nat.check(nat.lib().fsb_spmm_scratch_layout(nat.dtype_code(self.dtype), key, ctypes.byref(pb),
+                                                        ctypes.byref(tk)), "fsb_spmm_scratch_layout")
+            device = self.plan.units.device
+            slots = self.plan.n_slots
+            partials = torch.empty(max(slots * pb.value, 16), dtype=torch.uint8, device=device)
+            counters = torch.zeros(max(slots * tk.value, 1), dtype=torch.int32, device=device)
+            st = nat.SpmvPlan.from_buffer_copy(self.plan._struct)
+            st.partials = nat.ptr(partials)
+            st.counters = nat.ptr(counters)
+            entry = (partials, counters, st)
+            self._scratch[key] = entry
+        st = entry[2]
+        st.flags = nat.FSB_SPMM_COMPENSATED if compensated else 0
+        return ctypes.byref(st)
+
+    def counters_clear(self):
+        """True when every ticket is zero (the state each call must leave)."""
+        return all(int(c.abs().sum().item()) == 0 for _, c, _ in self._scratch.values())
+
+
+def spmm(data, indices, indptr, n_rows, n_cols, B, plan, out, compensated=False):
+    """out[:n_rows, :N] = A @ B through fsb_spmm_csr.
+
+    ``indices`` int32, ``indptr`` int64, ``B`` and ``out`` row-major 2-D with
+    unit column stride; ``plan`` a SpmmPlan of this matrix.
+    """
+    n = int(B.shape[1])
+    nat.check(
+        nat.lib().fsb_spmm_csr(
+            nat.dtype_code(data.dtype), nat.ptr(data), nat.ptr(indices), nat.ptr(indptr), int(n_rows), int(n_cols),
+            nat.ptr(B), int(B.stride(0)) if B.shape[0] > 1 else max(n, 1), n, nat.ptr(out),
+            int(out.stride(0)) if out.shape[0] > 1 else max(n, 1), plan.struct_for(n, compensated),
+            nat.stream_of(out.device),
+        ),
+        "fsb_spmm_csr",
+    )
+    return out

@@ -53,8 +53,14 @@ def distinct_sorted_columns(rng, lengths, n_cols):
     n_rows = lengths.size
     indptr = np.zeros(n_rows + 1, dtype=np.int64)
     np.cumsum(lengths, out=indptr[1:])
-    nnz = int(indptr[-1])
-    row_of = np.repeat(np.arange(n_rows, dtype=np.int64), lengths)
+    # Rows holding more than a quarter of the columns would make the redraw
+    # loop a coupon-collector run; they are drawn without replacement after
+    # the others (no such row exists in the full-size workloads, so their
+    # draws are unaffected).
+    dense = lengths > n_cols // 4
+    sparse_len = np.where(dense, 0, lengths)
+    nnz = int(sparse_len.sum())
+    row_of = np.repeat(np.arange(n_rows, dtype=np.int64), sparse_len)
     key = row_of * n_cols + rng.integers(0, n_cols, nnz, dtype=np.int64)
     key.sort()
     while True:
@@ -63,7 +69,14 @@ def distinct_sorted_columns(rng, lengths, n_cols):
             break
         key[dup] = row_of[dup] * n_cols + rng.integers(0, n_cols, dup.size, dtype=np.int64)
         key.sort()
-    cols = (key - row_of * n_cols).astype(np.int32)
+    sparse_cols = (key - row_of * n_cols).astype(np.int32)
+    if not dense.any():
+        return indptr, sparse_cols
+    cols = np.empty(int(indptr[-1]), dtype=np.int32)
+    is_sparse_pos = np.repeat(~dense, lengths)
+    cols[is_sparse_pos] = sparse_cols
+    for r in np.nonzero(dense)[0]:
+        cols[indptr[r]:indptr[r + 1]] = np.sort(rng.choice(n_cols, int(lengths[r]), replace=False))
     return indptr, cols
 
 
@@ -80,7 +93,7 @@ def poisson_csr(n=4096, mean=16.0, seed=0, dtype=np.float32):
 def zipf_csr(n=2_000_000, scale=ZIPF_SCALE_MEAN20, seed=1, dtype=np.float32, values="uniform"):
     """Configurations 2 and 3: square power-law CSR with sorted distinct columns."""
     rng = _rng(seed)
-    lengths = zipf_lengths(rng, n, scale)
+    lengths = zipf_lengths(rng, n, scale, cap=min(ZIPF_CAP, n))
     indptr, indices = distinct_sorted_columns(rng, lengths, n)
     if values == "uniform":
         data = rng.uniform(-1.0, 1.0, indices.size).astype(dtype)

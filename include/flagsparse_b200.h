@@ -207,6 +207,59 @@ FSB_API int fsb_spmv_csr_static_scratch(int dtype, const void* data, const void*
                                 const void* indptr, int ptr_is_64, int64_t n_rows, int64_t n_cols,
                                 const void* x, void* y, const fsb_spmv_plan* plan, void* stream);
 
+/* ------------------------------------------------------------------------
+ * CSR SpMM  C = A B  (A: n_rows x n_cols CSR with int32 column indices and
+ * int64 row pointers; B: n_cols x n row-major with row stride ldb; C: n_rows x
+ * n row-major with row stride ldc; every element of C is written).
+ *
+ * Uses an fsb_spmv_plan built by fsb_spmv_plan_analyze / _build with
+ * cap = fsb_spmm_default_cap (<= 64) and chunk_nnz = fsb_spmm_default_chunk
+ * (a multiple of 128).  One warp handles one (unit, column tile); lanes own
+ * consecutive column groups, with 16-byte loads where B, C, ldb and ldc are
+ * aligned for them.  Rows of several chunks reduce through the plan's
+ * scratch, sized per slot by fsb_spmm_scratch_layout for this n:
+ * partials = n_slots * partial_bytes_per_slot bytes, counters = n_slots *
+ * tickets_per_slot int32 (zero before the first call; left zero).
+ * Accumulation: fp32 for f16 / bf16 / f32, fp64 for f64, componentwise for
+ * complex; plan->flags & FSB_SPMM_COMPENSATED selects Dot2 compensated sums.
+ * Results are bitwise reproducible.
+ * Replaces _triton_spmm_csr_impl / _spmm_csr_real_kernel and the complex
+ * kernel (sparse_operations/spmm_csr.py:3373-3466, 144-339), which
+ * flagsparse_spmm_csr (spmm_csr.py:3981-4137) and every registered route
+ * (spmm_csr.py:2452-2544) launch.
+ * ------------------------------------------------------------------------ */
+#define FSB_SPMM_COMPENSATED 2
+
+FSB_API int32_t fsb_spmm_default_cap(int dtype);
+FSB_API int32_t fsb_spmm_default_chunk(int dtype);
+FSB_API int fsb_spmm_scratch_layout(int dtype, int64_t n, int64_t* partial_bytes_per_slot,
+                            int64_t* tickets_per_slot);
+FSB_API int fsb_spmm_csr(int dtype, const void* data, const int32_t* indices, const int64_t* indptr,
+                 int64_t n_rows, int64_t n_cols, const void* B, int64_t ldb, int64_t n,
+                 void* C, int64_t ldc, const fsb_spmv_plan* plan, void* stream);
+
+/* ------------------------------------------------------------------------
+ * CSR SDDMM  out[p] = alpha * <x[row(p)], y[col(p)]> + beta * in[p].
+ *
+ * x: M x k row-major (row stride ldx); y: N x k row-major (row stride ldy);
+ * row_ids / indices: int32[nnz] row and column of every nonzero (CSR order);
+ * in: nnz values or NULL (then beta is ignored); out: nnz values.  dtype is
+ * f16, bf16, f32 or f64; the dot products accumulate in fp32 (fp64 for f64)
+ * in a fixed order, or in fp64 with FSB_SDDMM_ACC64; FSB_SDDMM_OUT64 (with
+ * ACC64) writes fp64 results.  Each warp owns 32 nonzeros and reduces four
+ * dot products at a time.
+ * Replaces _sddmm_csr_real_kernel / _run_sddmm_prepared
+ * (sparse_operations/sddmm_csr.py:121-162, 291-384); fsb_csr_row_ids
+ * replaces _build_row_ids (sddmm_csr.py:95-104).
+ * ------------------------------------------------------------------------ */
+FSB_API int fsb_csr_row_ids(const void* indptr, int ptr_is_64, int64_t n_rows, int64_t nnz,
+                    int32_t* row_ids, void* stream);
+#define FSB_SDDMM_ACC64 1
+#define FSB_SDDMM_OUT64 2
+FSB_API int fsb_sddmm_csr(int dtype, const int32_t* row_ids, const int32_t* indices, int64_t nnz,
+                  const void* x, int64_t ldx, const void* y, int64_t ldy, int64_t k,
+                  const void* in, double alpha, double beta, void* out, int flags, void* stream);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

@@ -23,6 +23,16 @@ UNIT = {
     "float64": 2.0**-53,
     "complex128": 2.0**-53,
 }
+# half the smallest subnormal of the output dtype: the absolute error that
+# rounding a result into the subnormal range can add (Higham, sec. 2.1)
+ETA = {
+    "float16": 2.0**-25,
+    "bfloat16": 2.0**-134,
+    "float32": 2.0**-150,
+    "complex64": 2.0**-150,
+    "float64": 0.0,
+    "complex128": 0.0,
+}
 # unit roundoff of the accumulation type
 ACC_UNIT = {
     "float16": 2.0**-24,
@@ -67,7 +77,7 @@ def spmv_error_bound(dname, ref, scale, row_len):
     u, ua = UNIT[dname], ACC_UNIT[dname]
     n = 4.0 * np.maximum(np.asarray(row_len, dtype=np.float64), 1.0) + 8.0
     gamma = n * ua / (1.0 - n * ua)
-    return (u + 2.0 * ua) * np.abs(ref) + gamma * gamma * scale + 1e-300
+    return (u + 2.0 * ua) * np.abs(ref) + gamma * gamma * scale + ETA[dname] + 1e-300
 
 
 def assert_spmv_close(y, ref, scale, row_len, dname, what=""):
@@ -90,3 +100,28 @@ def op_csr(indptr, indices, data, shape, op):
     if op == "conj":
         d = np.conj(d)
     return t_ptr, t_idx, d, (shape[1], shape[0])
+
+
+def plain_error_bound(dname, ref, scale, n_terms):
+    """Bound for a working-precision sum of n products against the exact result:
+    |c - exact| <= u_out |exact| + gamma_n S, gamma_n = n u_acc / (1 - n u_acc),
+    S = sum |a||b| (Higham, Accuracy and Stability, eq. 3.5); complex products
+    count four terms."""
+    u, ua = UNIT[dname], ACC_UNIT[dname]
+    n = np.maximum(np.asarray(n_terms, dtype=np.float64), 1.0)
+    if dname.startswith("complex"):
+        n = 4.0 * n
+    n = n + 2.0
+    gamma = n * ua / (1.0 - n * ua)
+    return 2.0 * u * np.abs(ref) + gamma * scale + ETA[dname] + 1e-300
+
+
+def assert_within(got, ref, bound, what=""):
+    got = np.asarray(got)
+    if np.iscomplexobj(ref) or np.iscomplexobj(got):
+        err = np.maximum(np.abs(np.real(got) - np.real(ref)), np.abs(np.imag(got) - np.imag(ref)))
+    else:
+        err = np.abs(got - ref)
+    bad = np.argwhere(err > bound)
+    assert bad.size == 0, (f"{what}: {len(bad)} entries out of bound, first {bad[:3].tolist()}, "
+                           f"err {err[tuple(bad[:3].T)]}, bound {np.broadcast_to(bound, err.shape)[tuple(bad[:3].T)]}")

@@ -1,0 +1,121 @@
+"""Differentiable CSR SpMM: gradients against finite differences and the oracle."""
+
+import numpy as np
+import pytest
+import torch
+
+import flagsparse_b200 as fs
+from flagsparse_b200 import workloads
+from oracle import oracle
+from tests.helpers import dev, host, op_csr
+
+pytestmark = pytest.mark.gpu
+
+
+def _graph(n, seed=3):
+    g = workloads.chung_lu_graph(n=n, mean_degree=25.0, seed=seed)
+    return g["indptr"], g["indices"], g["data"].astype(np.float64), g["shape"]
+
+
+def test_gradcheck_float64_small():
+    mat = workloads.mask_csr(12, 9, seed=1, dtype=np.float64, long_rows=(4,))
+    p = fs.prepare_spmm_csr_autograd(dev(mat["data"]), dev(mat["indices"]), dev(mat["indptr"]), mat["shape"])
+    vals = dev(mat["data"]).requires_grad_(True)
+    X = torch.randn(9, 3, dtype=torch.float64, device="cuda", requires_grad=True)
+    assert torch.autograd.gradcheck(lambda v, x: fs.flagsparse_spmm_csr_autograd(v, x, prepared=p), (vals, X),
+                                    eps=1e-6, atol=1e-9, rtol=1e-7)
+
+
+def test_directional_finite_differences_chung_lu_1000():
+    """Central differences of L = <G, A(v) X> along 8 random directions, float64."""
+    indptr, indices, data, shape = _graph(1000)
+    p = fs.prepare_spmm_csr_autograd(dev(data), dev(indices), dev(indptr), shape)
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    vals = dev(data).requires_grad_(True)
+    X = torch.randn(1000, 16, dtype=torch.float64, device="cuda", generator=gen, requires_grad=True)
+    G = torch.randn(1000, 16, dtype=torch.float64, device="cuda", generator=gen)
+    loss = (fs.flagsparse_spmm_csr_autograd(vals, X, prepared=p) * G).sum()
+    gv, gx = torch.autograd.grad(loss, (vals, X))
+
+    def L(v, x):
+        return float((fs.flagsparse_spmm_csr_autograd(v, x, prepared=p) * G).sum())
+
+    h = 1e-5
+    for _ in range(8):
+        dv = torch.randn(vals.shape, dtype=torch.float64, device="cuda", generator=gen)
+        dx = torch.randn(X.shape, dtype=torch.float64, device="cuda", generator=gen)
+        with torch.no_grad():
+            fd = (L(vals + h * dv, X + h * dx) - L(vals - h * dv, X - h * dx)) / (2 * h)
+        an = float((gv * dv).sum() + (gx * dx).sum())
+        assert abs(fd - an) <= 1e-7 * max(1.0, abs(an)), (fd, an)
+
+
+def _oracle_grads(indptr, indices, vals, X, G, shape):
+    t_ptr, t_idx, t_vals, _ = op_csr(indptr, indices, vals, shape, "trans")
+    dX = oracle.spmm(t_ptr, t_idx, t_vals, G)
+    dv = oracle.sddmm(indptr, indices, G, X)
+    Y = oracle.spmm(indptr, indices, vals, X)
+    return Y, dX, dv
+
+
+def _rel(got, ref):
+    return float(np.max(np.abs(got - ref)) / max(np.max(np.abs(ref)), 1e-300))
+
+
+@pytest.mark.parametrize("dname,thresh", [("float64", 1e-12), ("float32", 1e-6), ("bfloat16", 1e-2),
+                                          ("float16", 5e-3)])
+def test_forward_backward_against_oracle(dname, thresh):
+    """Max relative error (FlagSparse's _spmm_relative_threshold metric) of Y, dX and dvals
+    against the fp64 oracle on the same rounded inputs."""
+    indptr, indices, data, shape = _graph(20_000, seed=4)
+    dt = getattr(torch, dname)
+    gen = torch.Generator(device="cuda").manual_seed(1)
+    vals = dev(data, dt).requires_grad_(True)
+    X = torch.randn(shape[1], 64, device="cuda", generator=gen).to(dt).requires_grad_(True)
+    G = torch.randn(shape[0], 64, device="cuda", generator=gen).to(dt)
+    p = fs.prepare_spmm_csr_autograd(vals.detach(), dev(indices), dev(indptr), shape)
+    Y = fs.flagsparse_spmm_csr_autograd(vals, X, prepared=p)
+    Y.backward(G)
+    Yo, dXo, dvo = _oracle_grads(indptr, indices, host(vals).astype(np.float64), host(X).astype(np.float64),
+                                 host(G).astype(np.float64), shape)
+    assert _rel(host(Y).astype(np.float64), Yo) <= thresh
+    assert _rel(host(X.grad).astype(np.float64), dXo) <= thresh
+    assert _rel(host(vals.grad).astype(np.float64), dvo) <= thresh
+
+
+def test_values_change_between_steps():
+    """The cached transpose regathers values every backward."""
+    indptr, indices, data, shape = _graph(2000, seed=5)
+    p = fs.prepare_spmm_csr_autograd(dev(data), dev(indices), dev(indptr), shape)
+    X = torch.randn(shape[1], 8, dtype=torch.float64, device="cuda", requires_grad=True)
+    for scale in (1.0, -3.0):
+        v = dev(data * scale)
+        G = torch.ones(shape[0], 8, dtype=torch.float64, device="cuda")
+        X.grad = None
+        fs.flagsparse_spmm_csr_autograd(v, X, prepared=p).backward(G)
+        _, dXo, _ = _oracle_grads(indptr, indices, data * scale, host(X), host(G), shape)
+        np.testing.assert_allclose(host(X.grad), dXo, rtol=1e-12, atol=1e-12)
+
+
+def test_autograd_full_size_bf16_sampled():
+    """500,000-node Chung-Lu graph, 128 features, bfloat16: forward + backward run, sampled rows of dX
+    within FlagSparse's bfloat16 threshold of the fp64 result."""
+    indptr, indices, data, shape = _graph(500_000)
+    gen = torch.Generator(device="cuda").manual_seed(2)
+    vals = dev(data, torch.bfloat16).requires_grad_(True)
+    X = torch.randn(shape[1], 128, device="cuda", generator=gen).bfloat16().requires_grad_(True)
+    p = fs.prepare_spmm_csr_autograd(vals.detach(), dev(indices), dev(indptr), shape)
+    Y = fs.flagsparse_spmm_csr_autograd(vals, X, prepared=p)
+    G = torch.randn(Y.shape, device="cuda", generator=gen).bfloat16()
+    Y.backward(G)
+    rows = np.sort(np.random.Generator(np.random.PCG64(6)).choice(shape[0], 500, replace=False))
+    lens = np.diff(indptr)[rows]
+    sub_ptr = np.zeros(rows.size + 1, dtype=np.int64)
+    np.cumsum(lens, out=sub_ptr[1:])
+    take = np.concatenate([np.arange(indptr[r], indptr[r + 1]) for r in rows])
+    v64 = host(vals).astype(np.float64)
+    # the graph is symmetric with symmetric values, so A^T rows equal A rows
+    dX_ref = oracle.spmm(sub_ptr, indices[take], v64[take], host(G).astype(np.float64))
+    got = host(X.grad[torch.from_numpy(rows).cuda()]).astype(np.float64)
+    assert _rel(got, dX_ref) <= 1e-2
+    assert torch.isfinite(vals.grad.float()).all()
