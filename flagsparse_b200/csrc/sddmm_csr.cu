@@ -10,6 +10,9 @@
 // together with a transpose butterfly (6 shuffles for 4 results instead of
 // 20).  Consecutive nonzeros mostly share a row, so the x slice is an L1 hit.
 //
+// That generic kernel serves every shape; rows of 5 to 64 aligned 16-byte
+// slices take the team kernel below, which caches the x row per team.
+//
 // Accumulation: fp32 for half / bfloat16 / fp32, fp64 for fp64 (fp64 for every
 // type with FSB_SDDMM_ACC64, which the reference's "acc64" variants select),
 // in a fixed order, so results are bitwise reproducible.
@@ -134,6 +137,200 @@ k_sddmm_csr(const int32_t* __restrict__ row_ids, const int32_t* __restrict__ col
   }
 }
 
+// ---------------------------------------------------------------------------
+// Fast path: teams of T lanes (8, 16 or 32) own 16-byte slices of a K-row,
+// TILES (1 or 2) slices per lane, so T * VW * TILES >= K.  A team walks U = 4
+// consecutive nonzeros per round; it keeps its current x row in registers as
+// fp32 and reloads it only when the row changes, so each nonzero costs one
+// 16-byte y load per lane.  The four dot products are reduced across the team
+// by a transpose butterfly: after the T/2 step a lane holds 2 items, after
+// T/4 one, then log2(T/4) plain steps.
+// ---------------------------------------------------------------------------
+constexpr int kTeamU = 4;
+
+template <typename S> struct Widen;
+template <> struct Widen<__nv_bfloat16> {
+  static constexpr int VW = 8;
+  __device__ __forceinline__ static void run(const uint4& w, float (&f)[8]) {
+    const unsigned u[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      f[2 * i] = __uint_as_float(u[i] << 16);
+      f[2 * i + 1] = __uint_as_float(u[i] & 0xffff0000u);
+    }
+  }
+};
+template <> struct Widen<__half> {
+  static constexpr int VW = 8;
+  __device__ __forceinline__ static void run(const uint4& w, float (&f)[8]) {
+    const unsigned u[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      __half2 h;
+      memcpy(&h, &u[i], 4);
+      const float2 p = __half22float2(h);
+      f[2 * i] = p.x;
+      f[2 * i + 1] = p.y;
+    }
+  }
+};
+template <> struct Widen<float> {
+  static constexpr int VW = 4;
+  __device__ __forceinline__ static void run(const uint4& w, float (&f)[4]) {
+    f[0] = __uint_as_float(w.x); f[1] = __uint_as_float(w.y);
+    f[2] = __uint_as_float(w.z); f[3] = __uint_as_float(w.w);
+  }
+};
+template <> struct Widen<double> {
+  static constexpr int VW = 2;
+  __device__ __forceinline__ static void run(const uint4& w, double (&f)[2]) {
+    f[0] = __hiloint2double(int(w.y), int(w.x));
+    f[1] = __hiloint2double(int(w.w), int(w.z));
+  }
+};
+
+// 16-byte slice at p, or only its first nv elements (the rest zero).
+template <typename S>
+__device__ __forceinline__ uint4 slice16(const S* p, int nv) {
+  constexpr int VW = 16 / int(sizeof(S));
+  if (nv == VW) return __ldg(reinterpret_cast<const uint4*>(p));
+  S tmp[VW];
+#pragma unroll
+  for (int j = 0; j < VW; ++j) {
+    if (j < nv) tmp[j] = p[j];
+    else memset(&tmp[j], 0, sizeof(S));
+  }
+  uint4 r;
+  memcpy(&r, tmp, 16);
+  return r;
+}
+
+template <int DT, int T, int TILES>
+__global__ void __launch_bounds__(kSddmmWarps * 32, TILES == 1 ? 4 : 3)
+k_sddmm_team(const int32_t* __restrict__ row_ids, const int32_t* __restrict__ col, int64_t nnz,
+             const typename VT<DT>::Store* __restrict__ x, int64_t ldx, const typename VT<DT>::Store* __restrict__ y,
+             int64_t ldy, int64_t k, const typename VT<DT>::Store* __restrict__ in, double alpha, double beta,
+             typename VT<DT>::Store* __restrict__ out) {
+  using S = typename VT<DT>::Store;
+  using R = typename VT<DT>::Real;
+  using W = Widen<S>;
+  constexpr int VW = W::VW;
+  constexpr int G = 32 / T;                 // teams per warp
+  constexpr int PER_ROUND = G * kTeamU;     // nonzeros per warp round
+  static_assert(T >= 8 && T <= 32, "team size");
+  const int lane = threadIdx.x & 31;
+  const int team = lane / T, tl = lane % T;
+  const int64_t base = (int64_t(blockIdx.x) * kSddmmWarps + (threadIdx.x >> 5)) * 32;
+  if (base >= nnz) return;  // whole warp leaves together
+  const int cnt = nnz - base < 32 ? static_cast<int>(nnz - base) : 32;
+  int my_r = -1, my_c = 0;
+  if (lane < cnt) {
+    my_r = __ldcs(row_ids + base + lane);
+    my_c = __ldcs(col + base + lane);
+  }
+  int nvt[TILES];
+  int64_t off[TILES];
+#pragma unroll
+  for (int t = 0; t < TILES; ++t) {
+    off[t] = (int64_t(t) * T + tl) * VW;
+    nvt[t] = static_cast<int>(k - off[t] >= VW ? int64_t(VW) : (k > off[t] ? k - off[t] : int64_t(0)));
+  }
+  const R a = static_cast<R>(alpha), b = static_cast<R>(beta);
+  int cur = -1;
+  R xf[TILES][VW];
+#pragma unroll
+  for (int t = 0; t < TILES; ++t)
+#pragma unroll
+    for (int j = 0; j < VW; ++j) xf[t][j] = R(0);
+
+  for (int r0 = 0; r0 < cnt; r0 += PER_ROUND) {
+    const int first = r0 + team * kTeamU;  // this team's items: first .. first+3
+    int rq[kTeamU], cq[kTeamU];
+#pragma unroll
+    for (int u = 0; u < kTeamU; ++u) {
+      rq[u] = __shfl_sync(0xffffffffu, my_r, (first + u) & 31);
+      cq[u] = __shfl_sync(0xffffffffu, my_c, (first + u) & 31);
+    }
+    uint4 yw[kTeamU][TILES];
+#pragma unroll
+    for (int u = 0; u < kTeamU; ++u) {
+      const bool valid = first + u < cnt;
+#pragma unroll
+      for (int t = 0; t < TILES; ++t)
+        yw[u][t] = slice16<S>(y + int64_t(cq[u]) * ldy + off[t], valid ? nvt[t] : 0);
+    }
+    R part[kTeamU];
+#pragma unroll
+    for (int u = 0; u < kTeamU; ++u) {
+      part[u] = R(0);
+      if (first + u < cnt) {
+        if (rq[u] != cur) {  // uniform inside the team
+          cur = rq[u];
+#pragma unroll
+          for (int t = 0; t < TILES; ++t) W::run(slice16<S>(x + int64_t(cur) * ldx + off[t], nvt[t]), xf[t]);
+        }
+#pragma unroll
+        for (int t = 0; t < TILES; ++t) {
+          R yf[VW];
+          W::run(yw[u][t], yf);
+#pragma unroll
+          for (int j = 0; j < VW; ++j) part[u] = fma(xf[t][j], yf[j], part[u]);
+        }
+      }
+    }
+    // transpose butterfly inside the team
+    constexpr int H = T / 2, Q = T / 4;
+    const bool hb = tl & H, qb = tl & Q;
+    R s0 = hb ? part[2] : part[0], s1 = hb ? part[3] : part[1];
+    const R o0 = hb ? part[0] : part[2], o1 = hb ? part[1] : part[3];
+    s0 += __shfl_xor_sync(0xffffffffu, o0, H);
+    s1 += __shfl_xor_sync(0xffffffffu, o1, H);
+    R v = qb ? s1 : s0;
+    v += __shfl_xor_sync(0xffffffffu, qb ? s0 : s1, Q);
+#pragma unroll
+    for (int m = Q / 2; m > 0; m >>= 1) v += __shfl_xor_sync(0xffffffffu, v, m);
+    const int item = first + (hb ? 2 : 0) + (qb ? 1 : 0);
+    if ((tl & (Q - 1)) == 0 && item < cnt) {
+      const int64_t p = base + item;
+      R res = v * a;
+      if (in) res += to_real(in[p]) * b;
+      out[p] = sddmm_out(res, out);
+    }
+  }
+}
+
+template <int DT, int T, int TILES>
+int sddmm_launch_team(const int32_t* row_ids, const int32_t* col, int64_t nnz, const void* x, int64_t ldx,
+                      const void* y, int64_t ldy, int64_t k, const void* in, double alpha, double beta, void* out,
+                      cudaStream_t st) {
+  using S = typename VT<DT>::Store;
+  const int64_t blocks = ceil_div(ceil_div(nnz, 32), kSddmmWarps);
+  if (blocks > INT32_MAX) return FSB_ERR_UNSUPPORTED;
+  k_sddmm_team<DT, T, TILES><<<(unsigned)blocks, kSddmmWarps * 32, 0, st>>>(
+      row_ids, col, nnz, static_cast<const S*>(x), ldx, static_cast<const S*>(y), ldy, k, static_cast<const S*>(in),
+      alpha, beta, static_cast<S*>(out));
+  FSB_LAUNCH_CHECK();
+  return FSB_OK;
+}
+
+// Fast path when x / y rows are 16-byte aligned and K fits two 16-byte
+// slices per lane of a 32-lane team; returns 1 when it launched (rc set).
+template <int DT>
+int sddmm_try_team(const int32_t* row_ids, const int32_t* col, int64_t nnz, const void* x, int64_t ldx,
+                   const void* y, int64_t ldy, int64_t k, const void* in, double alpha, double beta, void* out,
+                   int* rc, cudaStream_t st) {
+  using S = typename VT<DT>::Store;
+  constexpr int VW = 16 / int(sizeof(S));
+  if (reinterpret_cast<uintptr_t>(x) % 16 || reinterpret_cast<uintptr_t>(y) % 16 || ldx % VW || ldy % VW) return 0;
+  const int64_t slices = ceil_div(k, VW);  // 16-byte slices per row
+  if (slices < 5 || slices > 64) return 0;
+  if (slices <= 8) *rc = sddmm_launch_team<DT, 8, 1>(row_ids, col, nnz, x, ldx, y, ldy, k, in, alpha, beta, out, st);
+  else if (slices <= 16) *rc = sddmm_launch_team<DT, 16, 1>(row_ids, col, nnz, x, ldx, y, ldy, k, in, alpha, beta, out, st);
+  else if (slices <= 32) *rc = sddmm_launch_team<DT, 32, 1>(row_ids, col, nnz, x, ldx, y, ldy, k, in, alpha, beta, out, st);
+  else *rc = sddmm_launch_team<DT, 32, 2>(row_ids, col, nnz, x, ldx, y, ldy, k, in, alpha, beta, out, st);
+  return 1;
+}
+
 template <int DT, int V, bool ACC64, bool OUT64>
 int sddmm_launch_mode(const int32_t* row_ids, const int32_t* col, int64_t nnz, const void* x, int64_t ldx,
                       const void* y, int64_t ldy, int64_t k, const void* in, double alpha, double beta, void* out,
@@ -168,6 +365,10 @@ int sddmm_dispatch(const int32_t* row_ids, const int32_t* col, int64_t nnz, cons
                    int flags, cudaStream_t st) {
   using S = typename VT<DT>::Store;
   constexpr int kVmax = 16 / int(sizeof(S));
+  if (!(flags & (FSB_SDDMM_ACC64 | FSB_SDDMM_OUT64)) || DT == FSB_F64) {
+    int rc = FSB_OK;
+    if (sddmm_try_team<DT>(row_ids, col, nnz, x, ldx, y, ldy, k, in, alpha, beta, out, &rc, st)) return rc;
+  }
   int v = 1;
   while (v < kVmax && int64_t(32) * v < k) v *= 2;
   auto ok = [&](int w) {

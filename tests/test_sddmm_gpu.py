@@ -45,7 +45,7 @@ def test_sddmm_golden_cases(golden, shape, dname):
 
 
 @pytest.mark.parametrize("dname", ["float16", "bfloat16", "float32", "float64"])
-@pytest.mark.parametrize("K", [1, 7, 32, 64, 128, 130, 300])
+@pytest.mark.parametrize("K", [1, 7, 32, 64, 128, 130, 200, 256, 300])
 def test_sddmm_native_dtypes_and_widths(dname, K):
     """All value types the native kernel takes (the public API admits fp32 / fp64)."""
     indptr, indices, data = _pattern(40, 60, seed=K, long_rows=(2,))
