@@ -193,6 +193,261 @@ class SpmvZipf:
         return oracle.spmv_f32_acc64(c["indptr"], c["indices"], c["data"], c["x"], nthreads=nthreads)
 
 
+def _event_median_ms(torch, fn, flush, reps=10, warm=3):
+    """Median CUDA-event time of fn() with L2 flushed before every timed call."""
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for i in range(reps):
+        flush.fill_(float(i))
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        fn()
+        e.record()
+        torch.cuda.synchronize()
+        ts.append(s.elapsed_time(e))
+    return statistics.median(ts)
+
+
+def _sampled_rows(torch, c, n_sample, seed):
+    """n_sample random rows of c, the positions of their nonzeros, and each position's sample index."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    rows = np.sort(rng.choice(c["shape"][0], n_sample, replace=False))
+    ptr = c["indptr"]
+    take = np.concatenate([np.arange(ptr[r], ptr[r + 1]) for r in rows])
+    lens = np.diff(ptr)[rows]
+    owner = np.repeat(np.arange(rows.size), lens)
+    return rows, take, owner
+
+
+def _rows_fp64(torch, c, vals64, dense64, rows, take, owner):
+    """rows of A @ dense in float64 on the GPU (index_add over the sampled rows' nonzeros)."""
+    dev = dense64.device
+    cols = torch.from_numpy(c["indices"][take].astype(np.int64)).to(dev)
+    v = vals64[torch.from_numpy(take).to(dev)]
+    out = torch.zeros(rows.size, dense64.shape[1], dtype=torch.float64, device=dev)
+    out.index_add_(0, torch.from_numpy(owner).to(dev), v[:, None] * dense64[cols])
+    return out
+
+
+def _max_rel(got, ref):
+    return float((got - ref).abs().max() / ref.abs().max().clamp_min(1e-300))
+
+
+class SpmmPowerLaw:
+    """C = A B on the 1,000,000 x 1,000,000 power-law matrix (mean 29.7 per row, seed 2).
+
+    Bytes per step, gather model: nnz*(s_v+4) + (M+1)*8 + nnz*N*s + M*N*s (every
+    nonzero reads its B row; B exceeds L2).  The compulsory model (B once) is
+    reported beside it.
+    """
+
+    def __init__(self, device, dname="f32", n=128):
+        import torch
+
+        import flagsparse_b200 as fs
+        from flagsparse_b200 import workloads
+        from flagsparse_b200.sparse_operations import _csr
+
+        self.torch, self.fs, self._csr = torch, fs, _csr
+        self.dtype = dname
+        self.name = f"spmm_csr_powerlaw_1Mx1M_{dname}_N{n}"
+        dt = {"f32": torch.float32, "bf16": torch.bfloat16}[dname]
+        c = workloads.zipf_csr(n=1_000_000, scale=32.0 / workloads.ZIPF_MEAN_UNSCALED, seed=2, dtype=np.float32,
+                               values="normal")
+        self.host = c
+        self.M = self.K = c["shape"][0]
+        self.n = n
+        self.nnz = int(c["indices"].size)
+        self.vals = torch.from_numpy(c["data"]).to(device).to(dt)
+        self.ind = torch.from_numpy(c["indices"]).to(device)
+        self.ptr = torch.from_numpy(c["indptr"]).to(device)
+        g = torch.Generator(device=device).manual_seed(2)
+        self.B = torch.randn(self.K, n, device=device, generator=g).to(dt)
+        self.plan = _csr.SpmmPlan(self.ptr, self.M, dt)
+        self.C = torch.empty(self.M, n, dtype=dt, device=device)
+        self.route = fs.prepare_spmm_csr_route(self.vals, self.ind, self.ptr, c["shape"])
+        self.B_host = self.B.cpu().pin_memory()
+        self.C_host = torch.empty(self.M, n, dtype=dt).pin_memory()
+        self.B_dev2 = torch.empty_like(self.B)
+        self.s = self.B.element_size()
+
+    def config(self):
+        return {"workload": self.name, "rows": self.M, "cols": self.K, "nnz": self.nnz, "dense_cols": self.n,
+                "seed": 2, "l2": "flushed between timed steps (256 MiB write)"}
+
+    def alg_bytes(self):
+        s = self.s
+        return self.nnz * (s + 4) + (self.M + 1) * 8 + self.nnz * self.n * s + self.M * self.n * s
+
+    def compulsory_bytes(self):
+        s = self.s
+        return self.nnz * (s + 4) + self.K * self.n * s + self.M * self.n * s
+
+    def step(self):
+        self._csr.spmm(self.vals, self.ind, self.ptr, self.M, self.K, self.B, self.plan, self.C)
+
+    def e2e_step(self):
+        self.B_dev2.copy_(self.B_host, non_blocking=True)
+        C = self.fs.flagsparse_spmm_csr_run(self.route, self.B_dev2)
+        self.C_host.copy_(C, non_blocking=True)
+
+    def e2e_bytes(self):
+        return self.K * self.n * self.s, self.M * self.n * self.s
+
+    def max_rel_err(self, rows, take, owner):
+        torch = self.torch
+        ref = _rows_fp64(torch, self.host, self.vals.double(), self.B.double(), rows, take, owner)
+        return _max_rel(self.C[torch.from_numpy(rows).to(self.C.device)].double(), ref)
+
+
+class AutogradChungLu:
+    """Y = A X forward and dX = A^T dY, dvals = SDDMM(dY, X) backward on the 500,000-node
+    Chung-Lu graph (mean degree 25, seed 3), 128 features.
+
+    Bytes per step, gather model: forward and backward SpMM each
+    nnz*(s_v+4) + (n+1)*8 + nnz*128*s + n*128*s, plus the SDDMM
+    2*nnz*128*s + nnz*(4+4) + nnz*s.
+    """
+
+    def __init__(self, device, dname="bf16", part="fwd_bwd"):
+        import torch
+
+        import flagsparse_b200 as fs
+        from flagsparse_b200 import workloads
+        from flagsparse_b200.sparse_operations import sddmm_csr as dm
+
+        self.torch, self.fs, self.dm = torch, fs, dm
+        self.dtype = dname
+        self.part = part
+        self.name = f"autograd_spmm_chung_lu_500k_K128_{dname}" if part == "fwd_bwd" else \
+            f"sddmm_csr_chung_lu_500k_K128_{dname}"
+        dt = {"f32": torch.float32, "bf16": torch.bfloat16}[dname]
+        g = workloads.chung_lu_graph()
+        self.host = g
+        self.n = g["shape"][0]
+        self.nnz = int(g["indices"].size)
+        self.ind = torch.from_numpy(g["indices"]).to(device)
+        self.ptr = torch.from_numpy(g["indptr"]).to(device)
+        gen = torch.Generator(device=device).manual_seed(3)
+        self.vals = torch.from_numpy(g["data"]).to(device).to(dt).requires_grad_(True)
+        self.X = torch.randn(self.n, 128, device=device, generator=gen).to(dt).requires_grad_(True)
+        self.dY = torch.randn(self.n, 128, device=device, generator=gen).to(dt)
+        self.p = fs.prepare_spmm_csr_autograd(self.vals.detach(), self.ind, self.ptr, g["shape"])
+        self.out = torch.empty(self.nnz, dtype=dt, device=device)
+        self.s = self.X.element_size()
+        self.X_host = self.X.detach().cpu().pin_memory()
+        self.dY_host = self.dY.cpu().pin_memory()
+        self.g_host = torch.empty(self.nnz, dtype=dt).pin_memory()
+
+    def config(self):
+        return {"workload": self.name, "nodes": self.n, "nnz": self.nnz, "features": 128, "seed": 3,
+                "l2": "flushed between timed steps (256 MiB write)"}
+
+    def alg_bytes(self):
+        s, n, z = self.s, self.n, self.nnz
+        spmm = z * (s + 4) + (n + 1) * 8 + z * 128 * s + n * 128 * s
+        sddmm = 2 * z * 128 * s + z * 8 + z * s
+        return sddmm if self.part == "sddmm" else 2 * spmm + sddmm
+
+    def step(self):
+        if self.part == "sddmm":
+            self.dm._native_sddmm(self.p.row_ids, self.p.indices, self.dY, self.X.detach(), None, 1.0, 0.0, self.out)
+            return
+        self.vals.grad = None
+        self.X.grad = None
+        self.fs.flagsparse_spmm_csr_autograd(self.vals, self.X, prepared=self.p).backward(self.dY)
+
+    def e2e_step(self):
+        with self.torch.no_grad():
+            self.X.copy_(self.X_host, non_blocking=True)
+            self.dY.copy_(self.dY_host, non_blocking=True)
+        self.step()
+        grad = self.out if self.part == "sddmm" else self.vals.grad
+        self.g_host.copy_(grad, non_blocking=True)
+
+    def e2e_bytes(self):
+        return 2 * self.n * 128 * self.s, self.nnz * self.s
+
+    def max_rel_errs(self, rows, take, owner):
+        torch = self.torch
+        dev = self.X.device
+        self.vals.grad = None
+        self.X.grad = None
+        Y = self.fs.flagsparse_spmm_csr_autograd(self.vals, self.X, prepared=self.p)
+        Y.backward(self.dY)
+        sel = torch.from_numpy(rows).to(dev)
+        v64 = self.vals.detach().double()
+        g = self.host
+        # the graph and its values are symmetric, so rows of A^T equal rows of A
+        err_y = _max_rel(Y[sel].double(), _rows_fp64(torch, g, v64, self.X.detach().double(), rows, take, owner))
+        err_dx = _max_rel(self.X.grad[sel].double(), _rows_fp64(torch, g, v64, self.dY.double(), rows, take, owner))
+        tk = torch.from_numpy(take).to(dev)
+        r_ = torch.from_numpy(rows[owner].astype(np.int64)).to(dev)
+        c_ = torch.from_numpy(g["indices"][take].astype(np.int64)).to(dev)
+        dv_ref = (self.dY.double()[r_] * self.X.detach().double()[c_]).sum(1)
+        err_dv = _max_rel(self.vals.grad[tk].double(), dv_ref)
+        return {"max_rel_err_Y": err_y, "max_rel_err_dX": err_dx, "max_rel_err_dvals": err_dv}
+
+
+CASES = {
+    "spmm_f32_N64": lambda d: SpmmPowerLaw(d, "f32", 64),
+    "spmm_f32_N128": lambda d: SpmmPowerLaw(d, "f32", 128),
+    "spmm_bf16_N128": lambda d: SpmmPowerLaw(d, "bf16", 128),
+    "autograd_f32": lambda d: AutogradChungLu(d, "f32"),
+    "autograd_bf16": lambda d: AutogradChungLu(d, "bf16"),
+    "sddmm_f32_K128": lambda d: AutogradChungLu(d, "f32", part="sddmm"),
+    "sddmm_bf16_K128": lambda d: AutogradChungLu(d, "bf16", part="sddmm"),
+}
+
+
+# native kernels per step: the SpMM layer's backward gathers A^T's values,
+# runs the transposed SpMM and the SDDMM after the forward SpMM.
+LAUNCHES_PER_STEP = {"spmv": 1, "autograd_f32": 4, "autograd_bf16": 4}
+
+
+def measure_extras(torch, device, flush, peak):
+    """SpMM on the power-law matrix and the differentiable layer on the Chung-Lu graph:
+    CUDA-event medians (L2 flushed) and errors on sampled rows against float64 on the GPU."""
+    out = {}
+    spmm = {}
+    rows = take = owner = None
+    for key in ("spmm_f32_N64", "spmm_f32_N128", "spmm_bf16_N128"):
+        case = CASES[key](device)
+        if rows is None:
+            rows, take, owner = _sampled_rows(torch, case.host, 2000, 7)
+        ms = _event_median_ms(torch, case.step, flush)
+        gather, comp = case.alg_bytes(), case.compulsory_bytes()
+        spmm[key[5:]] = {"ms": round(ms, 4), "gather_model_gbs": round(gather / ms / 1e6, 1),
+                         "compulsory_model_gbs": round(comp / ms / 1e6, 1),
+                         "gather_model_frac": round(gather / ms / 1e6 / peak, 3),
+                         "max_rel_err_vs_fp64_sampled": case.max_rel_err(rows, take, owner)}
+        nnz, M = case.nnz, case.M
+        del case
+    out["spmm_powerlaw_1Mx1M"] = dict(spmm, nnz=nnz, rows=M, mean_row=round(nnz / M, 2),
+                                      bytes_models="gather: nnz*(s_v+4)+(M+1)*8+nnz*N*s+M*N*s; "
+                                                   "compulsory: nnz*(s_v+4)+K*N*s+M*N*s")
+    layer = {}
+    rows = None
+    for dname in ("f32", "bf16"):
+        case = AutogradChungLu(device, dname)
+        sd = AutogradChungLu.__new__(AutogradChungLu)
+        sd.__dict__.update(case.__dict__)
+        sd.part = "sddmm"
+        if rows is None:
+            rows, take, owner = _sampled_rows(torch, case.host, 500, 9)
+        ms = _event_median_ms(torch, case.step, flush)
+        ms_sd = _event_median_ms(torch, sd.step, flush)
+        layer[dname] = dict({"fwd_bwd_ms": round(ms, 4), "fwd_bwd_gather_model_gbs": round(case.alg_bytes() / ms / 1e6, 1),
+                             "sddmm_ms": round(ms_sd, 4)}, **case.max_rel_errs(rows, take, owner))
+        nnz = case.nnz
+        del case, sd
+    layer["bf16_speedup_vs_f32"] = round(layer["f32"]["fwd_bwd_ms"] / layer["bf16"]["fwd_bwd_ms"], 3)
+    out["autograd_chung_lu_500k_K128"] = dict(layer, nnz=nnz, error_reference="float64 on the GPU, 500 sampled rows")
+    return out
+
+
 def _cpu_measure(make_workload_host, budget_s, nthreads):
     """Repeat the CPU oracle over the whole matrix until ~budget_s seconds; return (s per step, reps)."""
     reps, t0 = 0, time.perf_counter()
@@ -214,6 +469,9 @@ def main():
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU-oracle work for cpu_baseline")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the SpMM and autograd measurements")
+    ap.add_argument("--case", default="spmv", choices=["spmv"] + sorted(CASES),
+                    help="workload of the timed steps (default: the SpMV headline)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -234,7 +492,8 @@ def main():
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=device)
 
-    wl = SpmvZipf(device)
+    wl = SpmvZipf(device) if args.case == "spmv" else CASES[args.case](device)
+    headline = args.case == "spmv"
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
 
     def barrier():
@@ -295,8 +554,12 @@ def main():
     traffic = _ncu_traffic(wl.name)
     h2d, d2h = wl.e2e_bytes()
 
+    extras = None
+    if world == 1 and headline and not args.no_extras:
+        extras = measure_extras(torch, device, flush, peak)
+
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+    if rank == 0 and world == 1 and headline and not args.no_cpu:
         from oracle import oracle
 
         nthreads = oracle.max_threads()
@@ -318,7 +581,8 @@ def main():
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": wl.dtype,
-            "data": "synthetic (seeded Zipf(2) power-law CSR, values/x U[-1,1])",
+            "data": ("synthetic (seeded Zipf(2) power-law CSR, values/x U[-1,1])" if headline
+                     else "synthetic (seeded generators; see config.workload)"),
             "config": dict(wl.config(), parallelism=f"replicas{world}" if world > 1 else "single"),
             "e2e": {"value": round(e2e_val, 2), "unit": "GB/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
@@ -327,8 +591,9 @@ def main():
                          "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs, copy burst)",
                          "alg_bytes_per_launch": alg},
             "cpu_baseline": cpu,
-            "gpu_launches": args.steps,
+            "gpu_launches": args.steps * LAUNCHES_PER_STEP.get(args.case, 1),
             "clocks": clocks,
+            "extras": extras,
         }
         print(json.dumps(line))
     if world > 1:
