@@ -46,6 +46,14 @@ def _measured_peaks():
     return 6650.0, "fallback"
 
 
+def _measured_bf16_tflops():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return float(json.load(f).get("bf16_tflops", 1590.0))
+    return 1590.0
+
+
 def _ncu_traffic(workload):
     path = os.path.join(REPO, "profiles", "ncu_traffic.json")
     if not os.path.exists(path):
@@ -391,7 +399,63 @@ class AutogradChungLu:
         return {"max_rel_err_Y": err_y, "max_rel_err_dX": err_dx, "max_rel_err_dvals": err_dv}
 
 
+class Bsr16:
+    """C = A B for the 16 x 16-block BSR matrix: 65,536 x 65,536 blocks (M = K = 1,048,576),
+    8 random distinct block columns per block row, bf16 values and B (N = 128), fp32
+    accumulation on the tensor cores (seed 2).
+
+    Bytes per step: nnzb*(512 + 4) + (n_brows+1)*8 + nnzb*16*N*2 (one B slab per
+    block) + M*N*2.  FLOPs per step: 2 * nnzb * 256 * N.
+    """
+
+    def __init__(self, device, n=128):
+        import torch
+
+        import flagsparse_b200 as fs
+        from flagsparse_b200 import workloads
+
+        self.torch, self.fs = torch, fs
+        self.dtype = "bf16"
+        self.name = f"bsr16_spmm_65536x65536_blocks_bf16_N{n}"
+        c = workloads.bsr16()
+        self.n_brows = c["block_shape"][0]
+        self.M = self.n_brows * 16
+        self.n = n
+        self.nnzb = int(c["indices"].size)
+        blocks = torch.from_numpy(c["blocks"]).to(device).to(torch.bfloat16)
+        self.p = fs.prepare_spmm_bsr16(blocks, torch.from_numpy(c["indices"]).to(device),
+                                       torch.from_numpy(c["indptr"]).to(device), (self.M, self.M))
+        g = torch.Generator(device=device).manual_seed(2)
+        self.B = torch.randn(self.M, n, device=device, generator=g).bfloat16()
+        self.C = torch.empty(self.M, n, dtype=torch.bfloat16, device=device)
+        self.B_host = self.B.cpu().pin_memory()
+        self.C_host = torch.empty(self.M, n, dtype=torch.bfloat16).pin_memory()
+        self.B_dev2 = torch.empty_like(self.B)
+
+    def config(self):
+        return {"workload": self.name, "block_rows": self.n_brows, "blocks_per_row": 8, "nnzb": self.nnzb,
+                "dense_cols": self.n, "seed": 2, "l2": "flushed between timed steps (256 MiB write)"}
+
+    def alg_bytes(self):
+        return self.nnzb * (512 + 4) + (self.n_brows + 1) * 8 + self.nnzb * 16 * self.n * 2 + self.M * self.n * 2
+
+    def flops(self):
+        return 2 * self.nnzb * 256 * self.n
+
+    def step(self):
+        self.fs.flagsparse_spmm_bsr16(B=self.B, prepared=self.p, out=self.C)
+
+    def e2e_step(self):
+        self.B_dev2.copy_(self.B_host, non_blocking=True)
+        self.fs.flagsparse_spmm_bsr16(B=self.B_dev2, prepared=self.p, out=self.C)
+        self.C_host.copy_(self.C, non_blocking=True)
+
+    def e2e_bytes(self):
+        return self.M * self.n * 2, self.M * self.n * 2
+
+
 CASES = {
+    "bsr16_bf16_N128": lambda d: Bsr16(d, 128),
     "spmm_f32_N64": lambda d: SpmmPowerLaw(d, "f32", 64),
     "spmm_f32_N128": lambda d: SpmmPowerLaw(d, "f32", 128),
     "spmm_bf16_N128": lambda d: SpmmPowerLaw(d, "bf16", 128),
@@ -445,6 +509,14 @@ def measure_extras(torch, device, flush, peak):
         del case, sd
     layer["bf16_speedup_vs_f32"] = round(layer["f32"]["fwd_bwd_ms"] / layer["bf16"]["fwd_bwd_ms"], 3)
     out["autograd_chung_lu_500k_K128"] = dict(layer, nnz=nnz, error_reference="float64 on the GPU, 500 sampled rows")
+    case = Bsr16(device)
+    ms = _event_median_ms(torch, case.step, flush)
+    bf16_peak = _measured_bf16_tflops()
+    out["bsr16_spmm_bf16_N128"] = {"ms": round(ms, 4), "gbs": round(case.alg_bytes() / ms / 1e6, 1),
+                                   "hbm_frac": round(case.alg_bytes() / ms / 1e6 / peak, 3),
+                                   "tflops": round(case.flops() / ms / 1e9, 1),
+                                   "tensor_frac_of_measured_bf16": round(case.flops() / ms / 1e9 / bf16_peak, 4),
+                                   "nnzb": case.nnzb, "bound": "hbm (12 flop/byte, far below the tensor ridge)"}
     return out
 
 

@@ -35,6 +35,10 @@ _OPS_EXPORTS = {
     "flagsparse_sddmm_csr",
     "list_spmm_csr_algorithms",
     "resolve_spmm_csr_algorithm",
+    # BSR-16 SpMM on the tensor cores (no FlagSparse counterpart)
+    "PreparedBsr16",
+    "prepare_spmm_bsr16",
+    "flagsparse_spmm_bsr16",
     # differentiable SpMM (no FlagSparse counterpart)
     "CsrSpmmFunction",
     "PreparedCsrSpmmAutograd",

@@ -112,6 +112,11 @@ _SIGNATURES = {
         [_c_int, _c_ptr, _c_ptr, _c_i64, _c_ptr, _c_i64, _c_ptr, _c_i64, _c_i64, _c_ptr,
          ctypes.c_double, ctypes.c_double, _c_ptr, _c_int, _c_ptr],
     ),
+    "fsb_bsr16_pack": (_c_int, [_c_int, _c_ptr, _c_i64, _c_ptr, _c_ptr]),
+    "fsb_bsr16_spmm": (
+        _c_int,
+        [_c_int, _c_ptr, _c_ptr, _c_ptr, _c_i64, _c_i64, _c_ptr, _c_i64, _c_i64, _c_ptr, _c_i64, _c_ptr, _c_ptr],
+    ),
     "fsb_spmv_csr_static_scratch": (
         _c_int,
         [_c_int, _c_ptr, _c_ptr, _c_int, _c_ptr, _c_int, _c_i64, _c_i64, _c_ptr, _c_ptr,

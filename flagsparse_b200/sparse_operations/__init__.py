@@ -2,7 +2,8 @@
 
 Mirrors the CSR hot-path part of FlagSparse ``sparse_operations/__init__.py``
 (``:18-137``, ``:149-268``): the same names, imported eagerly, plus the
-differentiable SpMM of ``autograd``.
+differentiable SpMM of ``autograd`` and the tensor-core BSR-16 SpMM of
+``bsr_spmm`` (neither has a FlagSparse counterpart).
 """
 
 from ._common import SUPPORTED_INDEX_DTYPES, SUPPORTED_VALUE_DTYPES
@@ -12,6 +13,7 @@ from .autograd import (
     flagsparse_spmm_csr_autograd,
     prepare_spmm_csr_autograd,
 )
+from .bsr_spmm import PreparedBsr16, flagsparse_spmm_bsr16, prepare_spmm_bsr16
 from .sddmm_csr import SDDMMPrepared, flagsparse_sddmm_csr, prepare_sddmm_csr
 from .spmm_csr import (
     SPMM_CSR_ALGORITHMS,
@@ -45,6 +47,7 @@ __all__ = [
     "SUPPORTED_VALUE_DTYPES",
     "SPMM_CSR_ALGORITHMS",
     "CsrSpmmFunction",
+    "PreparedBsr16",
     "PreparedCsrSpmmAutograd",
     "PreparedCsrSpmmOpt",
     "PreparedCsrSpmmOptAlg2",
@@ -54,6 +57,7 @@ __all__ = [
     "SpmmCsrAlgorithm",
     "SpmmCsrAlgorithmUnavailable",
     "flagsparse_sddmm_csr",
+    "flagsparse_spmm_bsr16",
     "flagsparse_spmm_csr",
     "flagsparse_spmm_csr_autograd",
     "flagsparse_spmm_csr_opt",
@@ -65,6 +69,7 @@ __all__ = [
     "flagsparse_spmv_csr",
     "list_spmm_csr_algorithms",
     "prepare_sddmm_csr",
+    "prepare_spmm_bsr16",
     "prepare_spmm_csr_autograd",
     "prepare_spmm_csr_opt",
     "prepare_spmm_csr_opt_alg1",

@@ -260,6 +260,26 @@ FSB_API int fsb_sddmm_csr(int dtype, const int32_t* row_ids, const int32_t* indi
                   const void* x, int64_t ldx, const void* y, int64_t ldy, int64_t k,
                   const void* in, double alpha, double beta, void* out, int flags, void* stream);
 
+/* ------------------------------------------------------------------------
+ * BSR SpMM with 16 x 16 blocks on the tensor cores (tcgen05.mma, fp32
+ * accumulation in tensor memory):  C = A B, A = n_brows x n_bcols blocks.
+ *
+ * fsb_bsr16_pack rearranges blocks ([nnzb][16][16] row-major, FSB_BF16 or
+ * FSB_F16) into the MMA's shared-memory layout, once per matrix; `packed`
+ * (same size, 16-byte aligned) is what fsb_bsr16_spmm reads.
+ * bcol: int32 block columns; bptr: int64 block row pointers [n_brows + 1];
+ * B: (16 n_bcols) x n row-major, row stride ldb, 16-byte aligned, read with
+ * TMA; C: (16 n_brows) x n, row stride ldc, written in the value type (block
+ * rows without blocks give zero rows).  n must be a multiple of 128 and ldb
+ * of 8.  d_error (device int) is set to 1 if a bounded wait inside the
+ * kernel expired.
+ * No FlagSparse counterpart: its BSR support is SpMV (spmv_bsr.py).
+ * ------------------------------------------------------------------------ */
+FSB_API int fsb_bsr16_pack(int dtype, const void* blocks, int64_t nnzb, void* packed, void* stream);
+FSB_API int fsb_bsr16_spmm(int dtype, const void* packed, const int32_t* bcol, const int64_t* bptr,
+                   int64_t n_brows, int64_t n_bcols, const void* B, int64_t ldb, int64_t n,
+                   void* C, int64_t ldc, int* d_error, void* stream);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif
