@@ -454,7 +454,72 @@ class Bsr16:
         return self.M * self.n * 2, self.M * self.n * 2
 
 
+class BatchedMix:
+    """256 CSR matrices, row counts log-uniform in [1,000, 200,000]: even ids 5-point stencils,
+    odd ids random with Poisson(24) rows; fp32, each with x and a 16-column B (seed 4).
+    A step is one CUDA-graph replay holding one SpMV and one SpMM over all 256 matrices
+    (block-diagonal combined plan, parameters chosen by the batch autotuner).
+
+    Bytes per step: the SpMV formula summed over matrices plus the SpMM compulsory model
+    (each B is at most 12.8 MB and stays in L2): sum nnz*(4+4)*2 + (rows+count)*8 + cols*4 +
+    rows*4 + cols*16*4 + rows*16*4.
+    """
+
+    def __init__(self, device):
+        import torch
+
+        import flagsparse_b200 as fs
+        from flagsparse_b200 import workloads
+
+        self.torch = torch
+        self.dtype = "f32"
+        self.name = "batched_256_uneven_f32_spmv_spmm16"
+        mats = workloads.batched_mix()
+        dev = [(torch.from_numpy(m["data"]).to(device), torch.from_numpy(m["indices"]).to(device),
+                torch.from_numpy(m["indptr"]).to(device), m["shape"]) for m in mats]
+        b = fs.BatchedCsr(dev, n_dense=16)
+        for i, m in enumerate(mats):
+            b.x_view(i).copy_(torch.from_numpy(m["x"]))
+            b.B_view(i).copy_(torch.from_numpy(m["B"]))
+        self.b = b
+        self.tuning = b.tune()
+        b.capture()
+        self.x_host = b.x.cpu().pin_memory()
+        self.B_host = b.B.cpu().pin_memory()
+        self.y_host = torch.empty(b.n_rows, dtype=torch.float32).pin_memory()
+        self.C_host = torch.empty(b.n_rows, 16, dtype=torch.float32).pin_memory()
+
+    def config(self):
+        b = self.b
+        return {"workload": self.name, "matrices": b.count, "rows": b.n_rows, "nnz": b.nnz, "dense_cols": 16,
+                "seed": 4, "schedule": {"spmv": b.spmv_cfg, "spmm": b.spmm_cfg,
+                                        "spmv_trials": self.tuning["spmv_trials"],
+                                        "spmm_trials": self.tuning["spmm_trials"]},
+                "launch": "one CUDA graph: SpMV + SpMM over the block-diagonal batch",
+                "l2": "flushed between timed steps (256 MiB write)"}
+
+    def alg_bytes(self):
+        spmv, spmm_c, _ = self.b.bytes_models()
+        return spmv + spmm_c
+
+    def step(self):
+        self.b.run()
+
+    def e2e_step(self):
+        b = self.b
+        b.x.copy_(self.x_host, non_blocking=True)
+        b.B.copy_(self.B_host, non_blocking=True)
+        b.run()
+        self.y_host.copy_(b.y, non_blocking=True)
+        self.C_host.copy_(b.C, non_blocking=True)
+
+    def e2e_bytes(self):
+        b = self.b
+        return (b.n_cols + b.n_cols * 16) * 4, (b.n_rows + b.n_rows * 16) * 4
+
+
 CASES = {
+    "batched_f32": lambda d: BatchedMix(d),
     "bsr16_bf16_N128": lambda d: Bsr16(d, 128),
     "spmm_f32_N64": lambda d: SpmmPowerLaw(d, "f32", 64),
     "spmm_f32_N128": lambda d: SpmmPowerLaw(d, "f32", 128),
@@ -468,7 +533,7 @@ CASES = {
 
 # native kernels per step: the SpMM layer's backward gathers A^T's values,
 # runs the transposed SpMM and the SDDMM after the forward SpMM.
-LAUNCHES_PER_STEP = {"spmv": 1, "autograd_f32": 4, "autograd_bf16": 4}
+LAUNCHES_PER_STEP = {"spmv": 1, "autograd_f32": 4, "autograd_bf16": 4, "batched_f32": 2}
 
 
 def measure_extras(torch, device, flush, peak):
@@ -509,6 +574,15 @@ def measure_extras(torch, device, flush, peak):
         del case, sd
     layer["bf16_speedup_vs_f32"] = round(layer["f32"]["fwd_bwd_ms"] / layer["bf16"]["fwd_bwd_ms"], 3)
     out["autograd_chung_lu_500k_K128"] = dict(layer, nnz=nnz, error_reference="float64 on the GPU, 500 sampled rows")
+    case = BatchedMix(device)
+    ms = _event_median_ms(torch, case.step, flush)
+    spmv_b, spmm_c, spmm_g = case.b.bytes_models()
+    out["batched_256_uneven_f32"] = {"ms": round(ms, 4), "gbs": round((spmv_b + spmm_c) / ms / 1e6, 1),
+                                     "gather_model_gbs": round((spmv_b + spmm_g) / ms / 1e6, 1),
+                                     "matrices": case.b.count, "rows": case.b.n_rows, "nnz": case.b.nnz,
+                                     "schedule": {"spmv": case.b.spmv_cfg, "spmm": case.b.spmm_cfg},
+                                     "launch": "one CUDA graph replay (SpMV + SpMM over all 256 matrices)"}
+    del case
     case = Bsr16(device)
     ms = _event_median_ms(torch, case.step, flush)
     bf16_peak = _measured_bf16_tflops()

@@ -35,6 +35,8 @@ _OPS_EXPORTS = {
     "flagsparse_sddmm_csr",
     "list_spmm_csr_algorithms",
     "resolve_spmm_csr_algorithm",
+    # batched uneven matrices in one graph launch (no FlagSparse counterpart)
+    "BatchedCsr",
     # BSR-16 SpMM on the tensor cores (no FlagSparse counterpart)
     "PreparedBsr16",
     "prepare_spmm_bsr16",

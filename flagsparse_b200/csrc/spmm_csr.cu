@@ -316,6 +316,159 @@ k_spmm_csr(const typename VT<DT>::Store* __restrict__ data, const int32_t* __res
   if (lane == 0) plan.counters[first * cps + tile] = 0;  // ready for the next call
 }
 
+// ---------------------------------------------------------------------------
+// Narrow dense rows (N * sizeof(value) <= 256 bytes): teams of T lanes own
+// 16-byte column slices and whole rows, G = 32 / T teams per warp.
+//  * row block: team g takes rows g, g+G, ... of the unit; the teams of a warp
+//    walk their rows together up to the longest of them (4 nonzeros ahead,
+//    inactive slots predicated off), so one load instruction moves G rows'
+//    B slices;
+//  * long-row chunk: team g takes nonzeros g, g+G, ...; the team partials are
+//    combined by xor-shuffles over the team index, then the chunk finishes as
+//    in k_spmm_csr (direct store or slot partial + ticket).
+// ---------------------------------------------------------------------------
+template <int DT, bool COMP, int V>
+__device__ __forceinline__ void acc_shfl_add(SpmmAcc<DT, COMP, V>& a, int m) {
+#pragma unroll
+  for (int c = 0; c < SpmmAcc<DT, COMP, V>::kNC; ++c)
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      const auto hi = __shfl_xor_sync(0xffffffffu, a.s[c][j].hi, m);
+      if constexpr (COMP) {
+        const auto lo = __shfl_xor_sync(0xffffffffu, a.s[c][j].lo, m);
+        a.s[c][j].add_comp(hi, lo);
+      } else {
+        a.s[c][j].add(hi);
+      }
+    }
+}
+
+template <int DT, bool COMP>
+__global__ void __launch_bounds__(kSpmmWarps * 32, SpmmMinBlocks<DT>::value)
+k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __restrict__ col,
+            const int64_t* __restrict__ ptr, const typename VT<DT>::Store* __restrict__ B, int64_t ldb, int64_t n,
+            typename VT<DT>::Store* __restrict__ C, int64_t ldc, fsb_spmv_plan plan, int T, int64_t pstride,
+            int64_t cps) {
+  using S = typename VT<DT>::Store;
+  using R = typename VT<DT>::Real;
+  constexpr int V = 16 / int(sizeof(S));
+  using Acc = SpmmAcc<DT, COMP, V>;
+  constexpr int kER = Acc::kNC * 2;
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t unit = int64_t(blockIdx.x) * kSpmmWarps + warp;
+  if (unit >= plan.n_units) return;  // whole warp leaves together
+  const int G = 32 / T, team = lane / T, tl = lane % T;
+  const int64_t c0 = int64_t(tl) * V;
+  const int nv = c0 + V <= n ? V : 0;  // n is a multiple of V
+
+  unsigned char* wbase = smem_raw + warp * spmm_warp_smem_bytes<S>();
+  S* sh_a = reinterpret_cast<S*>(wbase);
+  int32_t* sh_c = reinterpret_cast<int32_t*>(wbase + kSpmmBatch * sizeof(S));
+  int32_t* sh_off = sh_c + kSpmmBatch;
+
+  const fsb_spmv_unit* ud = plan.units + unit;
+  const int64_t s0 = __ldg(&ud->nnz_begin), s1 = __ldg(&ud->nnz_end);
+  const int32_t row = __ldg(&ud->row), tag = __ldg(&ud->tag);
+
+  if (tag >= 0) {
+    // ------------------------------------------------------------ row block
+    const int nr = tag - row;
+    const int cnt = static_cast<int>(s1 - s0);
+    for (int i = lane; i <= nr; i += 32) sh_off[i] = static_cast<int32_t>(__ldg(ptr + row + i) - s0);
+    for (int k = lane; k < cnt; k += 32) {
+      sh_a[k] = ld_once(data + s0 + k);
+      sh_c[k] = ld_once(col + s0 + k);
+    }
+    __syncwarp();
+    for (int i0 = 0; i0 < nr; i0 += G) {
+      const int i = i0 + team;
+      const bool has = i < nr;
+      const int b = has ? sh_off[i] : 0;
+      const int len = has ? sh_off[i + 1] - b : 0;
+      int maxlen = len;
+      for (int m = T; m < 32; m <<= 1) maxlen = max(maxlen, __shfl_xor_sync(0xffffffffu, maxlen, m));
+      Acc acc;
+      acc.zero();
+      for (int k = 0; k < maxlen; k += kSpmmAhead) {
+        S bv[kSpmmAhead][V];
+#pragma unroll
+        for (int u = 0; u < kSpmmAhead; ++u) {
+          const bool ok = k + u < len;
+          load_slice<S, V>(B + int64_t(sh_c[ok ? b + k + u : 0]) * ldb + c0, ok ? nv : 0, bv[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < kSpmmAhead; ++u)
+          if (k + u < len) acc.add(sh_a[b + k + u], bv[u]);
+      }
+      if (has && nv > 0) {
+        S o[V];
+        acc.result(o);
+        store_slice(C + (int64_t(row) + i) * ldc + c0, nv, o);
+      }
+    }
+    return;
+  }
+
+  // ------------------------------------------------------------ long-row chunk
+  const int32_t nch = __ldg(&ud->n_chunks), slot = __ldg(&ud->slot);
+  Acc acc;
+  acc.zero();
+  for (int64_t b0 = s0; b0 < s1; b0 += kSpmmBatch) {
+    const int cnt = static_cast<int>(s1 - b0 < kSpmmBatch ? s1 - b0 : int64_t(kSpmmBatch));
+    __syncwarp();
+    for (int k = lane; k < cnt; k += 32) {
+      sh_a[k] = ld_once(data + b0 + k);
+      sh_c[k] = ld_once(col + b0 + k);
+    }
+    __syncwarp();
+    for (int k = 0; k < cnt; k += kSpmmAhead * G) {
+      S bv[kSpmmAhead][V];
+#pragma unroll
+      for (int u = 0; u < kSpmmAhead; ++u) {
+        const int kk = k + u * G + team;
+        load_slice<S, V>(B + int64_t(sh_c[kk < cnt ? kk : 0]) * ldb + c0, kk < cnt ? nv : 0, bv[u]);
+      }
+#pragma unroll
+      for (int u = 0; u < kSpmmAhead; ++u) {
+        const int kk = k + u * G + team;
+        if (kk < cnt) acc.add(sh_a[kk], bv[u]);
+      }
+    }
+  }
+  for (int m = T; m < 32; m <<= 1) acc_shfl_add(acc, m);  // every team now holds the chunk's sum
+  if (nch == 1) {
+    if (team == 0 && nv > 0) {
+      S o[V];
+      acc.result(o);
+      store_slice(C + int64_t(row) * ldc + c0, nv, o);
+    }
+    return;
+  }
+  R* part = static_cast<R*>(plan.partials);
+  const int64_t first = int64_t(slot) + (tag + 1);
+  if (team == 0) acc.store_partial(part + (int64_t(slot) * pstride + c0) * kER);
+  __threadfence();
+  __syncwarp();
+  int ticket = 0;
+  if (lane == 0) ticket = atomicAdd(plan.counters + first * cps, 1);
+  ticket = __shfl_sync(0xffffffffu, ticket, 0);
+  if (ticket != nch - 1) return;
+  __threadfence();
+  if (team != 0) return;
+  Acc fin;
+  fin.zero();
+#pragma unroll 4
+  for (int c = 0; c < nch; ++c) fin.add_partial(part + ((first + c) * pstride + c0) * kER);
+  if (nv > 0) {
+    S o[V];
+    fin.result(o);
+    store_slice(C + int64_t(row) * ldc + c0, nv, o);
+  }
+  if (lane == 0) plan.counters[first * cps] = 0;  // ready for the next call
+}
+
 }  // namespace
 }  // namespace fsb
 
@@ -367,10 +520,30 @@ int spmm_pick_v(const void* B, int64_t ldb, const void* C, int64_t ldc, int64_t 
 }
 
 template <int DT, bool COMP>
+int spmm_launch_team(const void* data, const int32_t* idx, const int64_t* ptr, const void* B, int64_t ldb, int64_t n,
+                     void* C, int64_t ldc, const fsb_spmv_plan& plan, int T, cudaStream_t st) {
+  using S = typename VT<DT>::Store;
+  const int64_t blocks = ceil_div(plan.n_units, kSpmmWarps);
+  const size_t smem = size_t(spmm_warp_smem_bytes<S>()) * kSpmmWarps;
+  k_spmm_team<DT, COMP><<<(unsigned)blocks, kSpmmWarps * 32, smem, st>>>(
+      static_cast<const S*>(data), idx, ptr, static_cast<const S*>(B), ldb, n, static_cast<S*>(C), ldc, plan, T,
+      spmm_pstride(n), spmm_cps(n));
+  FSB_LAUNCH_CHECK();
+  return FSB_OK;
+}
+
+template <int DT, bool COMP>
 int spmm_dispatch(const void* data, const int32_t* idx, const int64_t* ptr, const void* B, int64_t ldb, int64_t n,
                   void* C, int64_t ldc, const fsb_spmv_plan& plan, cudaStream_t st) {
   using S = typename VT<DT>::Store;
   constexpr int kVmax = 16 / int(sizeof(S));
+  // narrow rows with whole, aligned 16-byte slices: teams of T lanes own rows
+  if (n * int64_t(sizeof(S)) <= 256 && n % kVmax == 0 && ldb % kVmax == 0 && ldc % kVmax == 0 &&
+      reinterpret_cast<uintptr_t>(B) % 16 == 0 && reinterpret_cast<uintptr_t>(C) % 16 == 0) {
+    int T = 1;
+    while (int64_t(T) * kVmax < n) T *= 2;
+    return spmm_launch_team<DT, COMP>(data, idx, ptr, B, ldb, n, C, ldc, plan, T, st);
+  }
   const int v = spmm_pick_v<DT>(B, ldb, C, ldc, n);
   if constexpr (kVmax >= 8)
     if (v == 8) return spmm_launch_v<DT, 8, COMP>(data, idx, ptr, B, ldb, n, C, ldc, plan, st);

@@ -413,7 +413,8 @@ static int spmv_launch_mode(const void* data, const void* idx, const void* ptr, 
 template <int DT, typename IT, typename PT>
 static int spmv_launch(const void* data, const void* idx, const void* ptr, const void* x, void* y,
                        const fsb_spmv_plan& plan, cudaStream_t st) {
-  if (plan.cap != kSpmvCap || plan.chunk_nnz % kSpmvBatch != 0) return FSB_ERR_INVALID_ARG;
+  // any window up to kSpmvCap fits a row-block unit's staging (<= cap rows, < 2*cap nonzeros)
+  if (plan.cap < 1 || plan.cap > kSpmvCap || plan.chunk_nnz % kSpmvBatch != 0) return FSB_ERR_INVALID_ARG;
   if (plan.flags & FSB_SPMV_FAST_SHORT_ROWS) return spmv_launch_mode<DT, IT, PT, false>(data, idx, ptr, x, y, plan, st);
   return spmv_launch_mode<DT, IT, PT, true>(data, idx, ptr, x, y, plan, st);
 }

@@ -3,7 +3,8 @@
 Mirrors the CSR hot-path part of FlagSparse ``sparse_operations/__init__.py``
 (``:18-137``, ``:149-268``): the same names, imported eagerly, plus the
 differentiable SpMM of ``autograd`` and the tensor-core BSR-16 SpMM of
-``bsr_spmm`` (neither has a FlagSparse counterpart).
+``bsr_spmm`` and the batched graph launch of ``batched`` (none has a
+FlagSparse counterpart).
 """
 
 from ._common import SUPPORTED_INDEX_DTYPES, SUPPORTED_VALUE_DTYPES
@@ -13,6 +14,7 @@ from .autograd import (
     flagsparse_spmm_csr_autograd,
     prepare_spmm_csr_autograd,
 )
+from .batched import BatchedCsr
 from .bsr_spmm import PreparedBsr16, flagsparse_spmm_bsr16, prepare_spmm_bsr16
 from .sddmm_csr import SDDMMPrepared, flagsparse_sddmm_csr, prepare_sddmm_csr
 from .spmm_csr import (
@@ -46,6 +48,7 @@ __all__ = [
     "SUPPORTED_INDEX_DTYPES",
     "SUPPORTED_VALUE_DTYPES",
     "SPMM_CSR_ALGORITHMS",
+    "BatchedCsr",
     "CsrSpmmFunction",
     "PreparedBsr16",
     "PreparedCsrSpmmAutograd",

@@ -190,12 +190,13 @@ class SpmmPlan:
     plus long-row scratch sized per dense width N (allocated once per N and
     reused; fsb_spmm_csr leaves the tickets zero after every call)."""
 
-    def __init__(self, indptr, n_rows, dtype):
+    def __init__(self, indptr, n_rows, dtype, cap=None, chunk_nnz=None):
         lib = nat.lib()
         code = nat.dtype_code(dtype)
         self.dtype = dtype
-        self.plan = NativeSpmvPlan(indptr, n_rows, dtype, cap=int(lib.fsb_spmm_default_cap(code)),
-                                   chunk_nnz=int(lib.fsb_spmm_default_chunk(code)), scratch=False)
+        cap = int(lib.fsb_spmm_default_cap(code)) if cap is None else int(cap)
+        chunk_nnz = int(lib.fsb_spmm_default_chunk(code)) if chunk_nnz is None else int(chunk_nnz)
+        self.plan = NativeSpmvPlan(indptr, n_rows, dtype, cap=cap, chunk_nnz=chunk_nnz, scratch=False)
         self._scratch = {}  # n -> (partials, counters, SpmvPlan struct)
 
     @property
