@@ -49,6 +49,7 @@ class SpmvPlan(ctypes.Structure):
         ("n_segs", _c_i64),
         ("n_units", _c_i64),
         ("n_slots", _c_i64),
+        ("n_block_units", _c_i64),
         ("cap", _c_i32),
         ("chunk_nnz", _c_i32),
         ("partials", _c_ptr),

@@ -73,15 +73,18 @@ static int inspect_impl(const void* idx, const void* ptr, int64_t n_rows, int64_
 // SpMV unit plan.  Row r starts a segment when it is long (len > cap), follows
 // a long row, is row 0, or when its window key (ptr[r] + r) / cap differs from
 // the previous row's.  A long segment is one row and owns ceil(len/chunk)
-// units; every other segment owns one unit.  Channel 0 counts segments,
-// channel 1 units, channel 2 scratch slots (one per chunk of a row of two or
-// more chunks: only those chunks publish a partial sum).
+// units; every other segment owns one row-block unit.  Row-block units come
+// first in the unit list (in row order), long-row chunks after them (in row
+// order), so the two kinds run as separate launches.  Channel 0 counts
+// segments, channel 1 row-block units, channel 2 scratch slots (one per chunk
+// of a row of two or more chunks: only those chunks publish a partial sum),
+// channel 3 long-row chunks.
 // ---------------------------------------------------------------------------
 template <typename PT>
 struct SpmvSegFlags {
   const PT* ptr;
   int64_t cap, chunk;
-  __device__ __forceinline__ Vec<3> operator()(int64_t r) const {
+  __device__ __forceinline__ Vec<4> operator()(int64_t r) const {
     int64_t a = ld_ptr(ptr, r), b = ld_ptr(ptr, r + 1);
     int64_t len = b - a;
     bool is_long = len > cap;
@@ -94,10 +97,11 @@ struct SpmvSegFlags {
       start = prev_long || ((pa + r - 1) / cap != (a + r) / cap);
     }
     const int64_t nch = is_long ? ceil_div(len, chunk) : 0;
-    Vec<3> v;
+    Vec<4> v;
     v.v[0] = start ? 1 : 0;
-    v.v[1] = is_long ? nch : (start ? 1 : 0);
+    v.v[1] = (start && !is_long) ? 1 : 0;
     v.v[2] = nch > 1 ? nch : 0;
+    v.v[3] = nch;
     return v;
   }
 };
@@ -111,13 +115,15 @@ struct SpmvSegWriter {
   int32_t* seg_row0;
   int32_t* seg_unit0;
   fsb_spmv_unit* units;
-  __device__ __forceinline__ void operator()(int64_t r, const Vec<3>& pre, const Vec<3>& val) const {
+  const int64_t* totals;  // scan totals: [1] = row-block units, which precede the long-row chunks
+  __device__ __forceinline__ void operator()(int64_t r, const Vec<4>& pre, const Vec<4>& val) const {
     if (val.v[0] == 0) return;
-    seg_row0[pre.v[0]] = static_cast<int32_t>(r);
-    seg_unit0[pre.v[0]] = static_cast<int32_t>(pre.v[1]);
     const int64_t a = ld_ptr(ptr, r), len = ld_ptr(ptr, r + 1) - a;
+    const int64_t first_unit = len <= cap ? pre.v[1] : totals[1] + pre.v[3];
+    seg_row0[pre.v[0]] = static_cast<int32_t>(r);
+    seg_unit0[pre.v[0]] = static_cast<int32_t>(first_unit);
     if (len <= cap) return;
-    const int32_t nch = static_cast<int32_t>(val.v[1]);
+    const int32_t nch = static_cast<int32_t>(val.v[3]);
     for (int32_t k = 0; k < nch; ++k) {
       fsb_spmv_unit d;
       d.nnz_begin = a + int64_t(k) * chunk;
@@ -126,14 +132,14 @@ struct SpmvSegWriter {
       d.tag = -(k + 1);
       d.n_chunks = nch;
       d.slot = nch > 1 ? static_cast<int32_t>(pre.v[2] + k) : -1;
-      units[pre.v[1] + k] = d;
+      units[first_unit + k] = d;
     }
   }
 };
 
 __global__ void k_spmv_plan_sentinel(const int64_t* totals, int64_t n_rows, int32_t* seg_row0, int32_t* seg_unit0) {
   seg_row0[totals[0]] = static_cast<int32_t>(n_rows);
-  seg_unit0[totals[0]] = static_cast<int32_t>(totals[1]);
+  seg_unit0[totals[0]] = static_cast<int32_t>(totals[1] + totals[3]);
 }
 
 // One thread per row-block segment writes that segment's descriptor.
@@ -158,9 +164,9 @@ __global__ void k_spmv_units(const PT* ptr, const int64_t* totals, const int32_t
 template <typename PT>
 static int spmv_plan_build_impl(const PT* ptr, int64_t n_rows, int64_t cap, int64_t chunk, const int64_t* ws,
                                 int32_t* seg_row0, int32_t* seg_unit0, fsb_spmv_unit* units, cudaStream_t st) {
-  const int64_t* totals = scan_totals<3>(ws, n_rows);
-  int rc = scan_apply<3>(SpmvSegFlags<PT>{ptr, cap, chunk}, SpmvSegWriter<PT>{ptr, cap, chunk, seg_row0, seg_unit0, units},
-                         n_rows, ws, st);
+  const int64_t* totals = scan_totals<4>(ws, n_rows);
+  int rc = scan_apply<4>(SpmvSegFlags<PT>{ptr, cap, chunk},
+                         SpmvSegWriter<PT>{ptr, cap, chunk, seg_row0, seg_unit0, units, totals}, n_rows, ws, st);
   if (rc != FSB_OK) return rc;
   k_spmv_plan_sentinel<<<1, 1, 0, st>>>(totals, n_rows, seg_row0, seg_unit0);
   FSB_LAUNCH_CHECK();
@@ -173,6 +179,16 @@ static int spmv_plan_build_impl(const PT* ptr, int64_t n_rows, int64_t cap, int6
 
 __global__ void k_copy_totals(const int64_t* src, int64_t* dst, int n) {
   if (threadIdx.x < n) dst[threadIdx.x] = src[threadIdx.x];
+}
+
+// public totals of the SpMV plan: n_segs, n_units, n_slots, n_block_units
+__global__ void k_spmv_totals(const int64_t* t, int64_t* out) {
+  if (threadIdx.x == 0) {
+    out[0] = t[0];
+    out[1] = t[1] + t[3];
+    out[2] = t[2];
+    out[3] = t[1];
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -362,13 +378,14 @@ int fsb_csr_inspect(const void* indices, int idx_is_64, const void* indptr, int 
                    : inspect_impl<int32_t, int32_t>(indices, indptr, n_rows, nnz, d_out, st);
 }
 
-// A row-block unit of a warp holds < 2*cap nonzeros, 8 per lane.
-int32_t fsb_spmv_default_cap(int dtype) { (void)dtype; return 128; }
+// A row-block unit of a warp holds < 2*cap nonzeros: 16 per lane for the 2- and
+// 4-byte real types (cap 256), 8 per lane for the wider types (cap 128).
+int32_t fsb_spmv_default_cap(int dtype) { return (dtype == FSB_F16 || dtype == FSB_BF16 || dtype == FSB_F32) ? 256 : 128; }
 
 // Long rows are cut into chunks of two 256-nonzero batches per warp.
 int32_t fsb_spmv_default_chunk(int dtype) { (void)dtype; return 512; }
 
-int64_t fsb_spmv_plan_workspace_bytes(int64_t n_rows) { return scan_workspace_bytes<3>(n_rows); }
+int64_t fsb_spmv_plan_workspace_bytes(int64_t n_rows) { return scan_workspace_bytes<4>(n_rows); }
 
 int fsb_spmv_plan_analyze(const void* indptr, int ptr_is_64, int64_t n_rows, int32_t cap, int32_t chunk_nnz,
                           void* workspace, int64_t workspace_bytes, int64_t* d_totals, void* stream) {
@@ -379,12 +396,12 @@ int fsb_spmv_plan_analyze(const void* indptr, int ptr_is_64, int64_t n_rows, int
   int64_t* ws = static_cast<int64_t*>(workspace);
   int rc;
   if (ptr_is_64) {
-    rc = scan_analyze<3>(SpmvSegFlags<int64_t>{static_cast<const int64_t*>(indptr), cap, chunk_nnz}, n_rows, ws, st);
+    rc = scan_analyze<4>(SpmvSegFlags<int64_t>{static_cast<const int64_t*>(indptr), cap, chunk_nnz}, n_rows, ws, st);
   } else {
-    rc = scan_analyze<3>(SpmvSegFlags<int32_t>{static_cast<const int32_t*>(indptr), cap, chunk_nnz}, n_rows, ws, st);
+    rc = scan_analyze<4>(SpmvSegFlags<int32_t>{static_cast<const int32_t*>(indptr), cap, chunk_nnz}, n_rows, ws, st);
   }
   if (rc != FSB_OK) return rc;
-  k_copy_totals<<<1, 32, 0, st>>>(scan_totals<3>(ws, n_rows), d_totals, 3);
+  k_spmv_totals<<<1, 32, 0, st>>>(scan_totals<4>(ws, n_rows), d_totals);
   FSB_LAUNCH_CHECK();
   return FSB_OK;
 }

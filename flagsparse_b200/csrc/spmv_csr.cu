@@ -182,9 +182,19 @@ template <> __device__ __forceinline__ __nv_bfloat16 ld_stream<__nv_bfloat16>(co
 template <typename T> __device__ __forceinline__ T ld_x(const T* p) { return __ldg(p); }
 
 constexpr int kSpmvWarps = 8;     // warps per block; one unit per warp
-constexpr int kSpmvItems = 8;     // nonzeros per lane per batch
+constexpr int kSpmvItems = 8;     // nonzeros per lane per long-row batch
 constexpr int kSpmvBatch = 32 * kSpmvItems;
-constexpr int kSpmvCap = kSpmvBatch / 2;  // row-block window: n < 2*cap <= batch
+
+// Row-block units: nonzero slots per lane.  A unit holds < 2*cap nonzeros, so
+// the largest window is cap = 16 * slots.  Units carry a fixed cost (their
+// descriptor, row-pointer and first loads are dependent round trips), so the
+// 2- and 4-byte real types use 16 slots (cap 256); the wider types keep 8.
+template <int DT>
+struct SpmvRow {
+  static constexpr int kItems = (DT == FSB_F16 || DT == FSB_BF16 || DT == FSB_F32) ? 16 : 8;
+  static constexpr int kBatch = 32 * kItems;
+  static constexpr int kCap = kBatch / 2;
+};
 
 struct UnitRegs { int64_t s0, s1; int32_t row, tag, nch, slot; };
 
@@ -207,7 +217,8 @@ template <int DT, bool SHORT_COMP>
 static constexpr int spmv_warp_smem_bytes() {
   using Tr = SpmvTraits<DT>;
   constexpr bool lo = SpmvAcc<DT, SHORT_COMP>::kLo;
-  return (Tr::kComp * int(sizeof(typename Tr::R)) * (lo ? 2 : 1) * kSpmvBatch + 4 * (kSpmvCap + 1) + 15) & ~15;
+  return (Tr::kComp * int(sizeof(typename Tr::R)) * (lo ? 2 : 1) * SpmvRow<DT>::kBatch + 4 * (SpmvRow<DT>::kCap + 1) +
+          15) & ~15;
 }
 
 // Resident blocks per SM the register budget is sized for: 8-byte reals and
@@ -215,11 +226,14 @@ static constexpr int spmv_warp_smem_bytes() {
 template <int DT>
 struct SpmvMinBlocks { static constexpr int value = (DT == FSB_C128) ? 2 : (DT == FSB_F64 || DT == FSB_C64) ? 3 : 4; };
 
-template <int DT, typename IT, typename PT, bool SHORT_COMP>
+// LONG = true: the long-row chunks units[unit0, unit1), no shared memory (the
+// gathers of long rows run faster with the L1 capacity that row-block staging
+// would take); LONG = false: the row-block units.
+template <int DT, typename IT, typename PT, bool SHORT_COMP, bool LONG>
 __global__ void __launch_bounds__(kSpmvWarps * 32, SpmvMinBlocks<DT>::value)
 k_spmv_csr(const typename VT<DT>::Store* __restrict__ data, const IT* __restrict__ col,
            const PT* __restrict__ ptr, const typename VT<DT>::Store* __restrict__ x,
-           typename VT<DT>::Store* __restrict__ y, fsb_spmv_plan plan) {
+           typename VT<DT>::Store* __restrict__ y, fsb_spmv_plan plan, int64_t unit0, int64_t unit1) {
   using Tr = SpmvTraits<DT>;
   using S = typename Tr::S;
   using R = typename Tr::R;
@@ -228,11 +242,11 @@ k_spmv_csr(const typename VT<DT>::Store* __restrict__ data, const IT* __restrict
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int64_t unit = int64_t(blockIdx.x) * kSpmvWarps + warp;
-  if (unit >= plan.n_units) return;  // whole warp leaves together
+  const int64_t unit = unit0 + int64_t(blockIdx.x) * kSpmvWarps + warp;
+  if (unit >= unit1) return;  // whole warp leaves together
   const UnitRegs u = load_unit(plan.units + unit);
 
-  if (u.tag < 0) {
+  if constexpr (LONG) {
     // ------------------------------------------------------ long-row chunk
     Acc acc;
     acc.zero();
@@ -295,9 +309,7 @@ k_spmv_csr(const typename VT<DT>::Store* __restrict__ data, const IT* __restrict
       y[u.row] = fin.result();
       plan.counters[s0] = 0;  // ready for the next call
     }
-    return;
-  }
-
+  } else {
   // -------------------------------------------------------------- row block
   using SAcc = SpmvAcc<DT, SHORT_COMP>;
   constexpr bool kLo = SAcc::kLo;
@@ -306,27 +318,32 @@ k_spmv_csr(const typename VT<DT>::Store* __restrict__ data, const IT* __restrict
   const int n = static_cast<int>(u.s1 - u.s0);
   unsigned char* wbase = smem_raw + warp * spmv_warp_smem_bytes<DT, SHORT_COMP>();
   R* sh_hi = reinterpret_cast<R*>(wbase);
-  R* sh_lo = sh_hi + NC * kSpmvBatch;
-  int32_t* sh_off = reinterpret_cast<int32_t*>(sh_hi + NC * kSpmvBatch * (kLo ? 2 : 1));
+  constexpr int kRowItems = SpmvRow<DT>::kItems, kRowBatch = SpmvRow<DT>::kBatch;
+  R* sh_lo = sh_hi + NC * kRowBatch;
+  int32_t* sh_off = reinterpret_cast<int32_t*>(sh_hi + NC * kRowBatch * (kLo ? 2 : 1));
 
-  S av[kSpmvItems];
-  IT cv[kSpmvItems];
+  // Units average about cap nonzeros against 2*cap slots: slots past n are
+  // skipped by a warp-uniform test instead of being issued predicated off.
+  S av[kRowItems];
+  IT cv[kRowItems];
 #pragma unroll
-  for (int k = 0; k < kSpmvItems; ++k) {
+  for (int k = 0; k < kRowItems; ++k) {
+    if (k * 32 >= n) break;
     const int i = k * 32 + lane;
     if (i < n) { av[k] = ld_stream(data + u.s0 + i); cv[k] = ld_stream(col + u.s0 + i); }
   }
   for (int i = lane; i <= nr; i += 32) sh_off[i] = static_cast<int32_t>(ld_ptr(ptr, r0 + i) - u.s0);
 #pragma unroll
-  for (int k = 0; k < kSpmvItems; ++k) {
+  for (int k = 0; k < kRowItems; ++k) {
+    if (k * 32 >= n) break;
     const int i = k * 32 + lane;
     if (i < n) {
       R hi[NC], lo[NC];
       SAcc::prod(av[k], ld_x(x + cv[k]), hi, lo);
 #pragma unroll
       for (int q = 0; q < NC; ++q) {
-        sh_hi[q * kSpmvBatch + i] = hi[q];
-        if constexpr (kLo) sh_lo[q * kSpmvBatch + i] = lo[q];
+        sh_hi[q * kRowBatch + i] = hi[q];
+        if constexpr (kLo) sh_lo[q * kRowBatch + i] = lo[q];
       }
     }
   }
@@ -366,8 +383,8 @@ k_spmv_csr(const typename VT<DT>::Store* __restrict__ data, const IT* __restrict
       R hi[NC], lo[NC];
 #pragma unroll
       for (int q = 0; q < NC; ++q) {
-        hi[q] = sh_hi[q * kSpmvBatch + j];
-        lo[q] = kLo ? sh_lo[q * kSpmvBatch + j] : R(0);
+        hi[q] = sh_hi[q * kRowBatch + j];
+        lo[q] = kLo ? sh_lo[q * kRowBatch + j] : R(0);
       }
       acc.add_rec(hi, lo);
       ++j;
@@ -390,31 +407,40 @@ k_spmv_csr(const typename VT<DT>::Store* __restrict__ data, const IT* __restrict
     if (lane > 0) first.combine(carry);
     y[r0 + first_row] = first.result();
   }
+  }  // row block
 }
 
 template <int DT, typename IT, typename PT, bool SHORT_COMP>
 static int spmv_launch_mode(const void* data, const void* idx, const void* ptr, const void* x, void* y,
                             const fsb_spmv_plan& plan, cudaStream_t st) {
   using S = typename VT<DT>::Store;
-  const size_t smem = size_t(spmv_warp_smem_bytes<DT, SHORT_COMP>()) * kSpmvWarps;
-  auto kern = k_spmv_csr<DT, IT, PT, SHORT_COMP>;
-  if (smem > 48 * 1024) {
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-      return FSB_ERR_CUDA;
+  const int64_t nb = plan.n_block_units, nu = plan.n_units;
+  if (nb > 0) {  // row blocks: per-warp staging in shared memory
+    const size_t smem = size_t(spmv_warp_smem_bytes<DT, SHORT_COMP>()) * kSpmvWarps;
+    auto kern = k_spmv_csr<DT, IT, PT, SHORT_COMP, false>;
+    if (smem > 48 * 1024) {
+      if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return FSB_ERR_CUDA;
+    }
+    kern<<<(unsigned)ceil_div(nb, kSpmvWarps), kSpmvWarps * 32, smem, st>>>(
+        static_cast<const S*>(data), static_cast<const IT*>(idx), static_cast<const PT*>(ptr),
+        static_cast<const S*>(x), static_cast<S*>(y), plan, 0, nb);
+    FSB_LAUNCH_CHECK();
   }
-  const int64_t blocks = ceil_div(plan.n_units, kSpmvWarps);
-  kern<<<(unsigned)blocks, kSpmvWarps * 32, smem, st>>>(static_cast<const S*>(data), static_cast<const IT*>(idx),
-                                                        static_cast<const PT*>(ptr), static_cast<const S*>(x),
-                                                        static_cast<S*>(y), plan);
-  FSB_LAUNCH_CHECK();
+  if (nu > nb) {  // long-row chunks: no shared memory
+    k_spmv_csr<DT, IT, PT, SHORT_COMP, true><<<(unsigned)ceil_div(nu - nb, kSpmvWarps), kSpmvWarps * 32, 0, st>>>(
+        static_cast<const S*>(data), static_cast<const IT*>(idx), static_cast<const PT*>(ptr),
+        static_cast<const S*>(x), static_cast<S*>(y), plan, nb, nu);
+    FSB_LAUNCH_CHECK();
+  }
   return FSB_OK;
 }
 
 template <int DT, typename IT, typename PT>
 static int spmv_launch(const void* data, const void* idx, const void* ptr, const void* x, void* y,
                        const fsb_spmv_plan& plan, cudaStream_t st) {
-  // any window up to kSpmvCap fits a row-block unit's staging (<= cap rows, < 2*cap nonzeros)
-  if (plan.cap < 1 || plan.cap > kSpmvCap || plan.chunk_nnz % kSpmvBatch != 0) return FSB_ERR_INVALID_ARG;
+  // any window up to the type's cap fits a row-block unit's staging (<= cap rows, < 2*cap nonzeros)
+  if (plan.cap < 1 || plan.cap > SpmvRow<DT>::kCap || plan.chunk_nnz % kSpmvBatch != 0) return FSB_ERR_INVALID_ARG;
   if (plan.flags & FSB_SPMV_FAST_SHORT_ROWS) return spmv_launch_mode<DT, IT, PT, false>(data, idx, ptr, x, y, plan, st);
   return spmv_launch_mode<DT, IT, PT, true>(data, idx, ptr, x, y, plan, st);
 }
@@ -489,6 +515,7 @@ int fsb_spmv_csr(int dtype, const void* data, const void* indices, int idx_is_64
   if (!plan || n_rows < 0 || n_cols < 0) return FSB_ERR_INVALID_ARG;
   if (n_rows == 0 || plan->n_units == 0) return FSB_OK;
   if (!indptr || !y || !plan->units || plan->cap < 1 || plan->chunk_nnz < 1 || plan->n_slots < 0 ||
+      plan->n_block_units < 0 || plan->n_block_units > plan->n_units ||
       (plan->n_slots > 0 && (!plan->partials || !plan->counters)))
     return FSB_ERR_INVALID_ARG;
   if (plan->n_units >= INT32_MAX) return FSB_ERR_UNSUPPORTED;

@@ -120,7 +120,7 @@ class NativeSpmvPlan:
     """Device arrays of the SpMV unit plan plus its scratch (see fsb_spmv_plan)."""
 
     __slots__ = ("seg_row0", "seg_unit0", "units", "partials", "counters", "cap", "chunk_nnz",
-                 "n_segs", "n_units", "n_slots", "dtype", "flags", "_struct")
+                 "n_segs", "n_units", "n_slots", "n_block_units", "dtype", "flags", "_struct")
 
     def __init__(self, indptr, n_rows, dtype, cap=None, chunk_nnz=None, fast_short_rows=False, scratch=True):
         lib = nat.lib()
@@ -133,14 +133,14 @@ class NativeSpmvPlan:
         st = nat.stream_of(device)
         ws_bytes = int(lib.fsb_spmv_plan_workspace_bytes(n_rows))
         ws = torch.empty(max(ws_bytes, 8), dtype=torch.uint8, device=device)
-        totals = torch.zeros(3, dtype=torch.int64, device=device)
+        totals = torch.zeros(4, dtype=torch.int64, device=device)
         if n_rows > 0:
             nat.check(
                 lib.fsb_spmv_plan_analyze(nat.ptr(indptr), nat.is64(indptr), n_rows, self.cap,
                                           self.chunk_nnz, nat.ptr(ws), ws_bytes, nat.ptr(totals), st),
                 "fsb_spmv_plan_analyze",
             )
-        self.n_segs, self.n_units, self.n_slots = (int(v) for v in totals.tolist())
+        self.n_segs, self.n_units, self.n_slots, self.n_block_units = (int(v) for v in totals.tolist())
         self.seg_row0 = torch.empty(self.n_segs + 1, dtype=torch.int32, device=device)
         self.seg_unit0 = torch.empty(self.n_segs + 1, dtype=torch.int32, device=device)
         # fsb_spmv_unit: int64 nnz_begin, nnz_end; int32 row, tag, n_chunks, slot (32 bytes)
@@ -162,7 +162,7 @@ class NativeSpmvPlan:
         self.flags = nat.FSB_SPMV_FAST_SHORT_ROWS if fast_short_rows else 0
         self._struct = nat.SpmvPlan(
             nat.ptr(self.seg_row0), nat.ptr(self.seg_unit0), nat.ptr(self.units),
-            self.n_segs, self.n_units, self.n_slots, self.cap, self.chunk_nnz,
+            self.n_segs, self.n_units, self.n_slots, self.n_block_units, self.cap, self.chunk_nnz,
             nat.ptr(self.partials), nat.ptr(self.counters), self.flags, 0,
         )
 

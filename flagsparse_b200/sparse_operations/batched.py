@@ -26,8 +26,10 @@ import torch
 from .. import _native as nat
 from . import _csr
 
-SPMV_CANDIDATES = ({"cap": 128, "chunk": 512}, {"cap": 64, "chunk": 512}, {"cap": 32, "chunk": 512},
-                   {"cap": 128, "chunk": 1024})
+# SpMV windows are given as fractions of the value type's largest window
+# (fsb_spmv_default_cap: 256 for 2- and 4-byte real types, 128 otherwise).
+SPMV_CANDIDATES = ({"cap": 1, "chunk": 512}, {"cap": 2, "chunk": 512}, {"cap": 4, "chunk": 512},
+                   {"cap": 1, "chunk": 1024})
 SPMM_CANDIDATES = ({"cap": 64, "chunk": 256}, {"cap": 32, "chunk": 256}, {"cap": 16, "chunk": 256},
                    {"cap": 64, "chunk": 512})
 _TUNE_CACHE = {}
@@ -81,7 +83,7 @@ class BatchedCsr:
         self.B = torch.zeros(self.n_cols, self.n_dense, dtype=dtype, device=device)
         self.y = torch.empty(self.n_rows, dtype=dtype, device=device)
         self.C = torch.empty(self.n_rows, self.n_dense, dtype=dtype, device=device)
-        self.spmv_cfg = dict(SPMV_CANDIDATES[0])
+        self.spmv_cfg = {"cap": int(nat.lib().fsb_spmv_default_cap(nat.dtype_code(dtype))), "chunk": 512}
         self.spmm_cfg = dict(SPMM_CANDIDATES[0])
         self._spmv_plan = self._spmm_plan = None
         self._graph = None
@@ -155,7 +157,9 @@ class BatchedCsr:
             return self.tuning
         report = {"signature": sig, "spmv_trials": [], "spmm_trials": []}
         best_v = best_m = None
-        for cfg in SPMV_CANDIDATES:
+        max_cap = int(nat.lib().fsb_spmv_default_cap(nat.dtype_code(self.dtype)))
+        for frac in SPMV_CANDIDATES:
+            cfg = {"cap": max_cap // frac["cap"], "chunk": frac["chunk"]}
             plan = _csr.NativeSpmvPlan(self.indptr, self.n_rows, self.dtype, cap=cfg["cap"], chunk_nnz=cfg["chunk"])
             ms = self._time(lambda: self._launch_spmv(plan))
             report["spmv_trials"].append(dict(cfg, ms=round(ms, 5)))

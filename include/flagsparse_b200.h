@@ -141,6 +141,8 @@ typedef struct fsb_spmv_plan {
   int64_t n_segs;
   int64_t n_units;
   int64_t n_slots;           /* scratch slots, see fsb_spmv_unit.slot                        */
+  int64_t n_block_units;     /* units[0, n_block_units) are row blocks, the rest long-row
+                                chunks (fsb_spmv_csr launches the two kinds separately)      */
   int32_t cap;               /* row-block window, see above                                  */
   int32_t chunk_nnz;         /* nonzeros per long-row chunk                                  */
   void* partials;            /* scratch: n_slots * fsb_spmv_partial_bytes(dtype) bytes       */
@@ -155,11 +157,13 @@ typedef struct fsb_spmv_plan {
  * compensated.  Off by default. */
 #define FSB_SPMV_FAST_SHORT_ROWS 1
 
+/* Row-block window: 256 for f16 / bf16 / f32 (16 nonzeros per lane), 128 for
+ * the wider types; any smaller window is accepted. */
 FSB_API int32_t fsb_spmv_default_cap(int dtype);
 FSB_API int32_t fsb_spmv_default_chunk(int dtype);
 FSB_API int64_t fsb_spmv_partial_bytes(int dtype);
 FSB_API int64_t fsb_spmv_plan_workspace_bytes(int64_t n_rows);
-/* d_totals (device int64[3]) receives n_segs, n_units and n_slots. */
+/* d_totals (device int64[4]) receives n_segs, n_units, n_slots and n_block_units. */
 FSB_API int fsb_spmv_plan_analyze(const void* indptr, int ptr_is_64, int64_t n_rows, int32_t cap,
                           int32_t chunk_nnz, void* workspace, int64_t workspace_bytes,
                           int64_t* d_totals, void* stream);

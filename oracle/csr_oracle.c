@@ -212,20 +212,24 @@ void oracle_bucketize(int64_t m, const int64_t* ptr, const int64_t* ub, int nb, 
 }
 
 /* ---- SpMV unit plan (segments, units) -------------------------------- */
-/* totals[0] = segments, totals[1] = units, totals[2] = scratch slots; arrays
- * may be NULL (count only).  Unit descriptors (when `units` != NULL) are 6
+/* totals[0] = segments, totals[1] = units, totals[2] = scratch slots,
+ * totals[3] = row-block units (they precede the long-row chunks); arrays may
+ * be NULL (count only).  Unit descriptors (when `units` != NULL) are 6
  * int64 per unit: nnz_begin, nnz_end, row, tag, n_chunks, slot (tag >= 0: row
  * block ending before row `tag`; tag < 0: chunk -(tag+1) of a long row; slot
  * numbers the chunks of rows of >= 2 chunks consecutively, -1 elsewhere). */
-void oracle_spmv_plan(int64_t m, const int64_t* ptr, int64_t cap, int64_t chunk, int64_t* totals, int32_t* seg_row0,
-                      int32_t* seg_unit0, int64_t* units) {
-  int64_t s = 0, u = 0, sl = 0;
+/* One sweep over the rows.  With nb >= 0 it writes: row-block units take
+ * indices [0, nb) in row order, long-row chunks [nb, nb + long units) in row
+ * order.  Returns the counts in out[0..3] = segments, row-block units, slots,
+ * long-row chunks. */
+static void spmv_plan_sweep(int64_t m, const int64_t* ptr, int64_t cap, int64_t chunk, int64_t nb, int32_t* seg_row0,
+                            int32_t* seg_unit0, int64_t* units, int64_t* out) {
+  int64_t s = 0, rb = 0, lg = 0, sl = 0;
   int64_t prev_start = -1;
   for (int64_t r = 0; r <= m; ++r) {
     int start = 0;
-    int64_t len = 0;
     if (r < m) {
-      len = ptr[r + 1] - ptr[r];
+      int64_t len = ptr[r + 1] - ptr[r];
       int is_long = len > cap;
       if (r == 0 || is_long) {
         start = 1;
@@ -241,9 +245,10 @@ void oracle_spmv_plan(int64_t m, const int64_t* ptr, int64_t cap, int64_t chunk,
         int64_t len0 = ptr[r0 + 1] - ptr[r0];
         if (r - r0 == 1 && len0 > cap) {
           int64_t nch = (len0 + chunk - 1) / chunk;
-          for (int64_t k = 0; k < nch; ++k) {
-            if (units) {
-              int64_t* d = units + 6 * (u + k);
+          if (nb >= 0) {
+            if (seg_unit0) seg_unit0[s - 1] = (int32_t)(nb + lg);
+            for (int64_t k = 0; k < nch && units; ++k) {
+              int64_t* d = units + 6 * (nb + lg + k);
               d[0] = ptr[r0] + k * chunk;
               d[1] = ptr[r0] + ((k + 1) * chunk < len0 ? (k + 1) * chunk : len0);
               d[2] = r0;
@@ -252,32 +257,48 @@ void oracle_spmv_plan(int64_t m, const int64_t* ptr, int64_t cap, int64_t chunk,
               d[5] = nch > 1 ? sl + k : -1;
             }
           }
-          u += nch;
+          lg += nch;
           if (nch > 1) sl += nch;
         } else {
-          if (units) {
-            int64_t* d = units + 6 * u;
-            d[0] = ptr[r0];
-            d[1] = ptr[r];
-            d[2] = r0;
-            d[3] = r;
-            d[4] = 1;
-            d[5] = -1;
+          if (nb >= 0) {
+            if (seg_unit0) seg_unit0[s - 1] = (int32_t)rb;
+            if (units) {
+              int64_t* d = units + 6 * rb;
+              d[0] = ptr[r0];
+              d[1] = ptr[r];
+              d[2] = r0;
+              d[3] = r;
+              d[4] = 1;
+              d[5] = -1;
+            }
           }
-          u += 1;
+          rb += 1;
         }
       }
       if (r < m) {
-        if (seg_row0) seg_row0[s] = (int32_t)r;
-        if (seg_unit0) seg_unit0[s] = (int32_t)u;
+        if (nb >= 0 && seg_row0) seg_row0[s] = (int32_t)r;
         s += 1;
         prev_start = r;
       }
     }
   }
-  if (seg_row0) seg_row0[s] = (int32_t)m;
-  if (seg_unit0) seg_unit0[s] = (int32_t)u;
-  totals[0] = s;
-  totals[1] = u;
-  totals[2] = sl;
+  if (nb >= 0) {
+    if (seg_row0) seg_row0[s] = (int32_t)m;
+    if (seg_unit0) seg_unit0[s] = (int32_t)(rb + lg);
+  }
+  out[0] = s;
+  out[1] = rb;
+  out[2] = sl;
+  out[3] = lg;
+}
+
+void oracle_spmv_plan(int64_t m, const int64_t* ptr, int64_t cap, int64_t chunk, int64_t* totals, int32_t* seg_row0,
+                      int32_t* seg_unit0, int64_t* units) {
+  int64_t cnt[4];
+  spmv_plan_sweep(m, ptr, cap, chunk, -1, NULL, NULL, NULL, cnt);
+  if (seg_row0 || seg_unit0 || units) spmv_plan_sweep(m, ptr, cap, chunk, cnt[1], seg_row0, seg_unit0, units, cnt);
+  totals[0] = cnt[0];
+  totals[1] = cnt[1] + cnt[3];
+  totals[2] = cnt[2];
+  totals[3] = cnt[1];
 }

@@ -186,7 +186,7 @@ def spmv_plan(indptr, cap, chunk):
     """
     ptr = _a(indptr, np.int64)
     m = ptr.size - 1
-    totals = np.zeros(3, dtype=np.int64)
+    totals = np.zeros(4, dtype=np.int64)
     lib().oracle_spmv_plan(m, _ptr(ptr), int(cap), int(chunk), _ptr(totals), None, None, None)
     s, u = int(totals[0]), int(totals[1])
     seg_row0 = np.empty(s + 1, dtype=np.int32)

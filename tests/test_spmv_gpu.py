@@ -127,6 +127,7 @@ def test_plan_and_buckets_bit_exact(n, seed):
         for got, exp in zip(plan.unit_table(), units.T):
             np.testing.assert_array_equal(got, exp)
         assert plan.n_slots == int(np.count_nonzero(units[:, 5] >= 0))
+        assert plan.n_block_units == int(np.count_nonzero(units[:, 3] >= 0))
     bounds = [64, 512, 4096, None]
     got = _csr.bucketize_rows(indptr, n, bounds)
     exp = oracle.bucketize(c["indptr"], bounds)
