@@ -20,6 +20,7 @@
 // Replaces _spmv_csr_real_kernel / _spmv_csr_complex_kernel
 // (sparse_operations/spmv_csr.py:179-240) and the bucketed CSR-vector kernels
 // (spmv_csr.py:247-368) of flagos-ai/FlagSparse.
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 #include <type_traits>
@@ -244,9 +245,9 @@ k_spmv_csr(const typename VT<DT>::Store* __restrict__ data, const IT* __restrict
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t unit = unit0 + int64_t(blockIdx.x) * kSpmvWarps + warp;
   if (unit >= unit1) return;  // whole warp leaves together
-  const UnitRegs u = load_unit(plan.units + unit);
 
   if constexpr (LONG) {
+    const UnitRegs u = load_unit(plan.units + unit);
     // ------------------------------------------------------ long-row chunk
     Acc acc;
     acc.zero();
@@ -311,6 +312,14 @@ k_spmv_csr(const typename VT<DT>::Store* __restrict__ data, const IT* __restrict
     }
   } else {
   // -------------------------------------------------------------- row block
+  // Persistent warps: units unit, unit + stride, ...; the next unit's
+  // descriptor is loaded while the current one is processed, so only the
+  // value / column loads and the x gathers remain on each unit's critical path.
+  const int64_t stride = int64_t(gridDim.x) * kSpmvWarps;
+  UnitRegs u = load_unit(plan.units + unit);
+  for (int64_t uid = unit; uid < unit1; uid += stride) {
+  UnitRegs nxt = u;
+  if (uid + stride < unit1) nxt = load_unit(plan.units + uid + stride);
   using SAcc = SpmvAcc<DT, SHORT_COMP>;
   constexpr bool kLo = SAcc::kLo;
   const int64_t r0 = u.row;
@@ -407,6 +416,9 @@ k_spmv_csr(const typename VT<DT>::Store* __restrict__ data, const IT* __restrict
     if (lane > 0) first.combine(carry);
     y[r0 + first_row] = first.result();
   }
+  __syncwarp();  // the staging slice is rewritten by the next unit
+  u = nxt;
+  }  // units of this warp
   }  // row block
 }
 
@@ -422,7 +434,9 @@ static int spmv_launch_mode(const void* data, const void* idx, const void* ptr, 
       if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return FSB_ERR_CUDA;
     }
-    kern<<<(unsigned)ceil_div(nb, kSpmvWarps), kSpmvWarps * 32, smem, st>>>(
+    // persistent: at most the resident blocks (SpmvMinBlocks per SM on 148 SMs)
+    const int64_t blocks = std::min<int64_t>(ceil_div(nb, kSpmvWarps), int64_t(148) * SpmvMinBlocks<DT>::value);
+    kern<<<(unsigned)blocks, kSpmvWarps * 32, smem, st>>>(
         static_cast<const S*>(data), static_cast<const IT*>(idx), static_cast<const PT*>(ptr),
         static_cast<const S*>(x), static_cast<S*>(y), plan, 0, nb);
     FSB_LAUNCH_CHECK();
