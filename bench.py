@@ -194,6 +194,11 @@ class SpmvZipf:
     def e2e_bytes(self):
         return self.K * 4, self.M * 4
 
+    def launches_per_step(self):
+        # row-block units and long-row chunks run as separate launches
+        p = self.prepared.native_plan()
+        return int(p.n_block_units > 0) + int(p.n_units > p.n_block_units)
+
     def cpu_run(self, nthreads):
         from oracle import oracle
 
@@ -517,6 +522,10 @@ class BatchedMix:
         b = self.b
         return (b.n_cols + b.n_cols * 16) * 4, (b.n_rows + b.n_rows * 16) * 4
 
+    def launches_per_step(self):
+        p = self.b._plans()[0]
+        return int(p.n_block_units > 0) + int(p.n_units > p.n_block_units) + 1
+
 
 CASES = {
     "batched_f32": lambda d: BatchedMix(d),
@@ -533,7 +542,7 @@ CASES = {
 
 # native kernels per step: the SpMM layer's backward gathers A^T's values,
 # runs the transposed SpMM and the SDDMM after the forward SpMM.
-LAUNCHES_PER_STEP = {"spmv": 1, "autograd_f32": 4, "autograd_bf16": 4, "batched_f32": 2}
+LAUNCHES_PER_STEP = {"autograd_f32": 4, "autograd_bf16": 4}
 
 
 def measure_extras(torch, device, flush, peak):
@@ -737,7 +746,8 @@ def main():
                          "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs, copy burst)",
                          "alg_bytes_per_launch": alg},
             "cpu_baseline": cpu,
-            "gpu_launches": args.steps * LAUNCHES_PER_STEP.get(args.case, 1),
+            "gpu_launches": args.steps * (wl.launches_per_step() if hasattr(wl, "launches_per_step")
+                                          else LAUNCHES_PER_STEP.get(args.case, 1)),
             "clocks": clocks,
             "extras": extras,
         }
