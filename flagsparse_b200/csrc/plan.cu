@@ -382,8 +382,10 @@ int fsb_csr_inspect(const void* indices, int idx_is_64, const void* indptr, int 
 // 4-byte real types (cap 256), 8 per lane for the wider types (cap 128).
 int32_t fsb_spmv_default_cap(int dtype) { return (dtype == FSB_F16 || dtype == FSB_BF16 || dtype == FSB_F32) ? 256 : 128; }
 
-// Long rows are cut into chunks of two 256-nonzero batches per warp.
-int32_t fsb_spmv_default_chunk(int dtype) { (void)dtype; return 512; }
+// Long rows are cut into chunks of 256-nonzero batches per warp: four for the
+// 2- and 4-byte real types (fewer tickets on the gather-bound long rows), two
+// for the wider types.
+int32_t fsb_spmv_default_chunk(int dtype) { return (dtype == FSB_F16 || dtype == FSB_BF16 || dtype == FSB_F32) ? 1024 : 512; }
 
 int64_t fsb_spmv_plan_workspace_bytes(int64_t n_rows) { return scan_workspace_bytes<4>(n_rows); }
 

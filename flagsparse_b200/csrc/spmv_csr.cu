@@ -1,21 +1,27 @@
 // CSR SpMV y = A x for sm_100a.
 //
-// One launch covers the whole matrix.  Every warp executes one work unit of
-// the plan built by fsb_spmv_plan_build (plan.cu); a unit's 32-byte
-// descriptor carries its nonzero range, so the warp issues its value / column
-// loads immediately, and the dozens of resident warps per SM keep many
-// independent load chains in flight:
+// Every warp executes work units of the plan built by fsb_spmv_plan_build
+// (plan.cu); a unit's 32-byte descriptor carries its nonzero range, so the
+// warp issues its value / column loads immediately.  The plan lists the two
+// kinds of unit apart, and each kind runs as its own launch:
 //
-//  * row-block unit: a run of rows with < 2*cap <= 256 nonzeros.  Lanes load
-//    8 nonzeros each with coalesced evict-first loads (x keeps its L2 lines),
+//  * row-block units: a run of rows with < 2*cap nonzeros.  Persistent warps
+//    stride over the units, loading the next unit's descriptor and
+//    prefetching its values and columns into L2 while the current unit runs.
+//    Lanes load up to 16 nonzeros each with coalesced evict-first loads,
 //    gather x, park the products in the warp's shared-memory slice in
-//    compensated form, and teams of T lanes (T ~ mean row length, <= 32) sum
-//    the rows and reduce with shuffles.
-//  * long-row chunk: `chunk_nnz` nonzeros of one row with > cap nonzeros, in
-//    256-nonzero batches whose loads are issued one batch ahead.  A one-chunk
-//    row is written directly; otherwise the warp publishes a partial sum and
-//    the warp whose atomic ticket completes the row adds all partials in a
-//    fixed order and resets the ticket, so results are deterministic.
+//    compensated form, then a lane-level merge path sums the rows and a
+//    segmented shuffle scan joins rows that span lanes.
+//  * long-row chunks: `chunk_nnz` nonzeros of one row with > cap nonzeros, in
+//    256-nonzero batches whose column loads are issued one batch ahead; no
+//    shared memory.  A one-chunk row is written directly; otherwise the warp
+//    publishes a partial sum and the warp whose atomic ticket completes the
+//    row adds all partials in a fixed order and resets the ticket, so results
+//    are deterministic.
+//
+// x is gathered with L2-only loads (ld.global.cg): the gathers have no reuse
+// in L1, and where the row-block staging takes most of L1 they run faster
+// without L1 allocation.
 //
 // Replaces _spmv_csr_real_kernel / _spmv_csr_complex_kernel
 // (sparse_operations/spmv_csr.py:179-240) and the bucketed CSR-vector kernels
@@ -180,7 +186,17 @@ template <> __device__ __forceinline__ __nv_bfloat16 ld_stream<__nv_bfloat16>(co
   unsigned short v = __ldcs(reinterpret_cast<const unsigned short*>(p));
   return __ushort_as_bfloat16(v);
 }
-template <typename T> __device__ __forceinline__ T ld_x(const T* p) { return __ldg(p); }
+// Gather of x: L2-only, no L1 allocation.
+template <typename T> __device__ __forceinline__ T ld_x(const T* p) { return __ldcg(p); }
+template <> __device__ __forceinline__ __half ld_x<__half>(const __half* p) {
+  return __ushort_as_half(__ldcg(reinterpret_cast<const unsigned short*>(p)));
+}
+template <> __device__ __forceinline__ __nv_bfloat16 ld_x<__nv_bfloat16>(const __nv_bfloat16* p) {
+  return __ushort_as_bfloat16(__ldcg(reinterpret_cast<const unsigned short*>(p)));
+}
+
+// One 128-byte line into L2; the address must lie inside the buffer.
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
 constexpr int kSpmvWarps = 8;     // warps per block; one unit per warp
 constexpr int kSpmvItems = 8;     // nonzeros per lane per long-row batch
@@ -226,12 +242,20 @@ static constexpr int spmv_warp_smem_bytes() {
 // complex values need more registers per thread than fp32 / half types.
 template <int DT>
 struct SpmvMinBlocks { static constexpr int value = (DT == FSB_C128) ? 2 : (DT == FSB_F64 || DT == FSB_C64) ? 3 : 4; };
+// The long-row kernel keeps fewer values live (no staging, columns one batch
+// ahead): the 2- and 4-byte real types with 32-bit columns fit 5 blocks per SM
+// without spills.
+template <int DT, typename IT>
+struct SpmvLongMinBlocks {
+  static constexpr int value =
+      ((DT == FSB_F16 || DT == FSB_BF16 || DT == FSB_F32) && sizeof(IT) == 4) ? 5 : SpmvMinBlocks<DT>::value;
+};
 
 // LONG = true: the long-row chunks units[unit0, unit1), no shared memory (the
 // gathers of long rows run faster with the L1 capacity that row-block staging
 // would take); LONG = false: the row-block units.
 template <int DT, typename IT, typename PT, bool SHORT_COMP, bool LONG>
-__global__ void __launch_bounds__(kSpmvWarps * 32, SpmvMinBlocks<DT>::value)
+__global__ void __launch_bounds__(kSpmvWarps * 32, LONG ? SpmvLongMinBlocks<DT, IT>::value : SpmvMinBlocks<DT>::value)
 k_spmv_csr(const typename VT<DT>::Store* __restrict__ data, const IT* __restrict__ col,
            const PT* __restrict__ ptr, const typename VT<DT>::Store* __restrict__ x,
            typename VT<DT>::Store* __restrict__ y, fsb_spmv_plan plan, int64_t unit0, int64_t unit1) {
@@ -249,36 +273,38 @@ k_spmv_csr(const typename VT<DT>::Store* __restrict__ data, const IT* __restrict
   if constexpr (LONG) {
     const UnitRegs u = load_unit(plan.units + unit);
     // ------------------------------------------------------ long-row chunk
+    // Offsets within the chunk are 32-bit (chunk_nnz < 2^31).  Columns run one
+    // batch ahead; values are loaded beside the x gathers they pair with.
     Acc acc;
     acc.zero();
-    S av[kSpmvItems];
+    const S* dp = data + u.s0;
+    const IT* cp = col + u.s0;
+    const int n = static_cast<int>(u.s1 - u.s0);
     IT cv[kSpmvItems];
 #pragma unroll
     for (int k = 0; k < kSpmvItems; ++k) {
-      const int64_t i = u.s0 + k * 32 + lane;
-      if (i < u.s1) { av[k] = ld_stream(data + i); cv[k] = ld_stream(col + i); }
+      const int i = k * 32 + lane;
+      if (i < n) cv[k] = ld_stream(cp + i);
     }
-    for (int64_t base = u.s0; base < u.s1; base += kSpmvBatch) {
-      S xv[kSpmvItems];
+    for (int base = 0; base < n; base += kSpmvBatch) {
+      S av[kSpmvItems], xv[kSpmvItems];
 #pragma unroll
       for (int k = 0; k < kSpmvItems; ++k) {
-        if (base + k * 32 + lane < u.s1) xv[k] = ld_x(x + cv[k]);
+        const int i = base + k * 32 + lane;
+        if (i < n) { xv[k] = ld_x(x + cv[k]); av[k] = ld_stream(dp + i); }
       }
-      // next batch's loads go out before this batch is summed
-      S an[kSpmvItems];
       IT cn[kSpmvItems];
-      const int64_t nb = base + kSpmvBatch;
 #pragma unroll
       for (int k = 0; k < kSpmvItems; ++k) {
-        const int64_t i = nb + k * 32 + lane;
-        if (i < u.s1) { an[k] = ld_stream(data + i); cn[k] = ld_stream(col + i); }
+        const int i = base + kSpmvBatch + k * 32 + lane;
+        if (i < n) cn[k] = ld_stream(cp + i);
       }
 #pragma unroll
       for (int k = 0; k < kSpmvItems; ++k) {
-        if (base + k * 32 + lane < u.s1) acc.add_prod(av[k], xv[k]);
+        if (base + k * 32 + lane < n) acc.add_prod(av[k], xv[k]);
       }
 #pragma unroll
-      for (int k = 0; k < kSpmvItems; ++k) { av[k] = an[k]; cv[k] = cn[k]; }
+      for (int k = 0; k < kSpmvItems; ++k) cv[k] = cn[k];
     }
 #pragma unroll
     for (int m = 16; m > 0; m >>= 1) acc.shfl_combine(m);
@@ -342,6 +368,20 @@ k_spmv_csr(const typename VT<DT>::Store* __restrict__ data, const IT* __restrict
     if (i < n) { av[k] = ld_stream(data + u.s0 + i); cv[k] = ld_stream(col + u.s0 + i); }
   }
   for (int i = lane; i <= nr; i += 32) sh_off[i] = static_cast<int32_t>(ld_ptr(ptr, r0 + i) - u.s0);
+  if (uid + stride < unit1) {
+    // the next unit's values (lanes 0-15) and columns (lanes 16-31) into L2,
+    // one line per lane: 16 lines of each cover a whole unit of the 2- and
+    // 4-byte types and the first part of a unit of the wider types
+    const int64_t nn = nxt.s1 - nxt.s0;
+    const int li = lane & 15;
+    if (lane < 16) {
+      constexpr int kPer = 128 / int(sizeof(S));
+      if (int64_t(li) * kPer < nn) prefetch_l2(data + nxt.s0 + int64_t(li) * kPer);
+    } else {
+      constexpr int kPer = 128 / int(sizeof(IT));
+      if (int64_t(li) * kPer < nn) prefetch_l2(col + nxt.s0 + int64_t(li) * kPer);
+    }
+  }
 #pragma unroll
   for (int k = 0; k < kRowItems; ++k) {
     if (k * 32 >= n) break;

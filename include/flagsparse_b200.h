@@ -160,6 +160,8 @@ typedef struct fsb_spmv_plan {
 /* Row-block window: 256 for f16 / bf16 / f32 (16 nonzeros per lane), 128 for
  * the wider types; any smaller window is accepted. */
 FSB_API int32_t fsb_spmv_default_cap(int dtype);
+/* Long-row chunk: 1024 nonzeros for f16 / bf16 / f32, 512 for the wider types;
+ * any positive multiple of 256 is accepted. */
 FSB_API int32_t fsb_spmv_default_chunk(int dtype);
 FSB_API int64_t fsb_spmv_partial_bytes(int dtype);
 FSB_API int64_t fsb_spmv_plan_workspace_bytes(int64_t n_rows);
