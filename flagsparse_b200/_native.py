@@ -83,6 +83,13 @@ _SIGNATURES = {
          _c_ptr, _c_int, _c_ptr, _c_int, _c_ptr, _c_ptr],
     ),
     "fsb_gather_values": (_c_int, [_c_int, _c_ptr, _c_ptr, _c_i64, _c_int, _c_ptr, _c_ptr]),
+    "fsb_coo_inspect": (_c_int, [_c_ptr, _c_int, _c_ptr, _c_int, _c_i64, _c_i64, _c_i64, _c_ptr, _c_ptr]),
+    "fsb_coo_to_csr_workspace_bytes": (_c_i64, [_c_i64, _c_i64, _c_i64]),
+    "fsb_coo_to_csr": (
+        _c_int,
+        [_c_ptr, _c_int, _c_ptr, _c_int, _c_i64, _c_i64, _c_i64, _c_int, _c_ptr, _c_i64, _c_ptr, _c_ptr, _c_ptr,
+         _c_ptr],
+    ),
     "fsb_spmv_default_cap": (_c_i32, [_c_int]),
     "fsb_spmv_default_chunk": (_c_i32, [_c_int]),
     "fsb_spmv_partial_bytes": (_c_i64, [_c_int]),

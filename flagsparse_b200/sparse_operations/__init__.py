@@ -42,7 +42,13 @@ from .spmm_csr_opt_alg2 import (
     prepare_spmm_csr_opt_alg2,
     prepare_spmm_csr_opt_alg2_preprocess,
 )
-from .spmv_csr import PreparedCsrSpmv, flagsparse_spmv_csr, prepare_spmv_csr
+from .spmv_csr import (
+    PreparedCsrSpmv,
+    flagsparse_spmv_coo_tocsr,
+    flagsparse_spmv_csr,
+    prepare_spmv_coo_tocsr,
+    prepare_spmv_csr,
+)
 
 __all__ = [
     "SUPPORTED_INDEX_DTYPES",
@@ -69,6 +75,7 @@ __all__ = [
     "flagsparse_spmm_csr_opt_alg2",
     "flagsparse_spmm_csr_opt_alg2_preprocess",
     "flagsparse_spmm_csr_run",
+    "flagsparse_spmv_coo_tocsr",
     "flagsparse_spmv_csr",
     "list_spmm_csr_algorithms",
     "prepare_sddmm_csr",
@@ -80,6 +87,7 @@ __all__ = [
     "prepare_spmm_csr_opt_alg2",
     "prepare_spmm_csr_opt_alg2_preprocess",
     "prepare_spmm_csr_route",
+    "prepare_spmv_coo_tocsr",
     "prepare_spmv_csr",
     "resolve_spmm_csr_algorithm",
 ]

@@ -73,6 +73,55 @@ def transpose_pattern(indices, indptr, shape, out_index_dtype, out_indptr_dtype)
     return t_indices, t_indptr, perm
 
 
+def coo_inspect(row, col, n_rows, n_cols):
+    """(pairs out of (row, col) order, rows outside [0, n_rows), columns outside [0, n_cols)).
+
+    One kernel, one device-to-host read.
+    """
+    out = torch.empty(3, dtype=torch.int64, device=row.device)
+    nnz = int(row.numel())
+    nat.check(
+        nat.lib().fsb_coo_inspect(
+            nat.ptr(row) if nnz else None, nat.is64(row), nat.ptr(col) if nnz else None, nat.is64(col), nnz,
+            int(n_rows), int(n_cols), nat.ptr(out), nat.stream_of(row.device),
+        ),
+        "fsb_coo_inspect",
+    )
+    unsorted, bad_rows, bad_cols = out.tolist()
+    return unsorted, bad_rows, bad_cols
+
+
+def coo_to_csr(row, col, n_rows, n_cols, ordered):
+    """CSR pattern of a COO pattern: ``(indices int32, indptr int64, perm)``.
+
+    ``ordered``: the pairs are already in (row, col) order; then ``perm`` is
+    None (identity).  Otherwise ``perm`` (int64) holds the source position of
+    every CSR entry, from a stable sort (repeated pairs keep their order).
+    """
+    nnz = int(row.numel())
+    device = row.device
+    indices = torch.empty(nnz, dtype=torch.int32, device=device)
+    indptr = torch.empty(int(n_rows) + 1, dtype=torch.int64, device=device)
+    lib = nat.lib()
+    perm = ws = None
+    ws_bytes = 0
+    if not ordered and nnz > 0:
+        ws_bytes = int(lib.fsb_coo_to_csr_workspace_bytes(nnz, int(n_rows), int(n_cols)))
+        if ws_bytes < 0:
+            raise RuntimeError("COO to CSR: nnz must be < 2^31")
+        ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=device)
+        perm = torch.empty(nnz, dtype=torch.int64, device=device)
+    nat.check(
+        lib.fsb_coo_to_csr(
+            nat.ptr(row) if nnz else None, nat.is64(row), nat.ptr(col) if nnz else None, nat.is64(col), nnz,
+            int(n_rows), int(n_cols), 1 if ordered else 0, nat.ptr(ws), ws_bytes, nat.ptr(indices) if nnz else None,
+            nat.ptr(indptr), nat.ptr(perm), nat.stream_of(device),
+        ),
+        "fsb_coo_to_csr",
+    )
+    return indices, indptr, perm
+
+
 def gather_values(values, perm, conj=False):
     """values[perm] (conjugated for complex when ``conj``), computed natively."""
     out = torch.empty(perm.numel(), dtype=values.dtype, device=values.device)

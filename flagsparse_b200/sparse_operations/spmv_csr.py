@@ -541,3 +541,144 @@ def flagsparse_spmv_csr(
     if return_time:
         return y, op_total_ms
     return y
+
+
+# ---------------------------------------------------------------------------
+# COO input: conversion to CSR feeding the CSR SpMV
+# (sparse_operations/spmv_csr.py:948-1091 of flagos-ai/FlagSparse).
+# ---------------------------------------------------------------------------
+def _coo_index(t):
+    """int32 / int64 index tensors pass through; other integer dtypes widen to int64."""
+    return t if t.dtype in (torch.int32, torch.int64) else t.to(torch.int64)
+
+
+def _coo_is_sorted_lex(row, col, n_cols):
+    """True iff the COO pairs are in non-decreasing (row, col) order."""
+    if row.numel() <= 1:
+        return True
+    unsorted, _, _ = _csr.coo_inspect(_coo_index(row).contiguous(), _coo_index(col).contiguous(), 2**31 - 1,
+                                      max(1, int(n_cols)))
+    return unsorted == 0
+
+
+def coo_to_csr_for_spmv(data, row, col, shape, assume_sorted=False):
+    """Convert COO to CSR triple (data, csr_col_indices, indptr) for SpMV.
+
+    Returns values in CSR order (``data`` itself when the pairs are already in
+    (row, col) order), int32 column indices and int64 row pointers.  The order
+    and the index ranges are checked natively in one pass; unordered input is
+    sorted even when ``assume_sorted`` is set.  Repeated (row, col) pairs are
+    kept as separate entries in their input order.
+    """
+    n_rows, n_cols = int(shape[0]), int(shape[1])
+    row = _coo_index(row).contiguous()
+    col = _coo_index(col).contiguous()
+    if row.numel() == 0:
+        indptr = torch.zeros(n_rows + 1, dtype=torch.int64, device=data.device)
+        return data, col.to(torch.int32), indptr
+    unsorted, bad_rows, bad_cols = _csr.coo_inspect(row, col, n_rows, n_cols)
+    if bad_rows:
+        raise RuntimeError(f"row indices out of range for n_rows={n_rows}")
+    if bad_cols:
+        raise IndexError("indices out of range for n_cols")
+    ordered = unsorted == 0
+    indices, indptr, perm = _csr.coo_to_csr(row, col, n_rows, n_cols, ordered)
+    data_s = data if ordered else _csr.gather_values(data.contiguous(), perm)
+    return data_s, indices, indptr
+
+
+def prepare_spmv_coo_tocsr(
+    data,
+    row,
+    col,
+    shape,
+    block_nnz=256,
+    max_segments=None,
+    assume_sorted=False,
+):
+    """One-time COO -> CSR + plan; use with ``flagsparse_spmv_coo_tocsr(..., prepared=p)``."""
+    if not all(torch.is_tensor(t) for t in (data, row, col)):
+        raise TypeError("data, row, col must all be torch.Tensor")
+    if not all(t.is_cuda for t in (data, row, col)):
+        raise ValueError("data, row, col must all be CUDA tensors")
+    if data.ndim != 1 or row.ndim != 1 or col.ndim != 1:
+        raise ValueError("data, row, col must all be 1D tensors")
+    if data.dtype not in SUPPORTED_SPMV_VALUE_DTYPES:
+        raise TypeError(_spmv_dtype_error_message())
+    if row.numel() != col.numel() or data.numel() != row.numel():
+        raise ValueError("data, row, col must have the same length")
+    data_s, indices, indptr = coo_to_csr_for_spmv(data, row, col, shape, assume_sorted=assume_sorted)
+    return prepare_spmv_csr(
+        data_s,
+        indices,
+        indptr,
+        shape,
+        block_nnz=block_nnz,
+        max_segments=max_segments,
+    )
+
+
+def flagsparse_spmv_coo_tocsr(
+    data=None,
+    row=None,
+    col=None,
+    x=None,
+    shape=None,
+    block_nnz=256,
+    max_segments=None,
+    out=None,
+    return_time=False,
+    use_opt=True,
+    prepared=None,
+    assume_sorted=False,
+):
+    """COO SpMV via CSR conversion: y = A @ x.
+
+    Steady state: ``p = prepare_spmv_coo_tocsr(data, row, col, shape)`` then
+    call with ``prepared=p`` (``data`` / ``row`` / ``col`` may be omitted).
+    ``use_opt`` is forwarded to flagsparse_spmv_csr (bucket lists in meta);
+    the native kernel is the same either way.
+    """
+    if prepared is not None:
+        if x is None:
+            raise TypeError("x is required")
+        if shape is None:
+            shape = prepared.shape
+        sh = (int(shape[0]), int(shape[1]))
+        if sh != prepared.shape:
+            raise ValueError(f"shape {sh} does not match prepared.shape {prepared.shape}")
+        return flagsparse_spmv_csr(
+            x=x,
+            shape=shape,
+            block_nnz=block_nnz,
+            max_segments=max_segments,
+            out=out,
+            return_time=return_time,
+            use_opt=use_opt,
+            prepared=prepared,
+        )
+
+    if not all(torch.is_tensor(t) for t in (data, row, col, x)):
+        raise TypeError("data, row, col, x must all be torch.Tensor")
+    if not all(t.is_cuda for t in (data, row, col, x)):
+        raise ValueError("data, row, col, x must all be CUDA tensors")
+    if data.ndim != 1 or row.ndim != 1 or col.ndim != 1 or x.ndim != 1:
+        raise ValueError("data, row, col, x must all be 1D tensors")
+    if data.dtype not in SUPPORTED_SPMV_VALUE_DTYPES:
+        raise TypeError(_spmv_dtype_error_message())
+    if x.dtype != data.dtype:
+        raise TypeError("x dtype must match data dtype")
+
+    data_s, indices, indptr = coo_to_csr_for_spmv(data, row, col, shape, assume_sorted=assume_sorted)
+    return flagsparse_spmv_csr(
+        data_s,
+        indices,
+        indptr,
+        x,
+        shape,
+        block_nnz=block_nnz,
+        max_segments=max_segments,
+        out=out,
+        return_time=return_time,
+        use_opt=use_opt,
+    )

@@ -104,6 +104,30 @@ FSB_API int fsb_gather_values(int dtype, const void* src, const int64_t* perm, i
                       void* dst, void* stream);
 
 /* ------------------------------------------------------------------------
+ * COO -> CSR, the on-ramp for COO inputs (replaces coo_to_csr_for_spmv and
+ * _coo_is_sorted_lex, sparse_operations/spmv_csr.py:948-984).
+ *
+ * fsb_coo_inspect: d_out (device int64[3]) receives the number of adjacent
+ * pairs out of (row, col) order, of rows outside [0, n_rows) and of columns
+ * outside [0, n_cols).
+ *
+ * fsb_coo_to_csr: out_col (int32[nnz]) and out_ptr (int64[n_rows + 1]) of
+ * the CSR with entries in (row, col) order.  sorted != 0 states that the
+ * input is already in that order (no workspace, perm untouched); otherwise a
+ * stable radix sort of the packed (row, col) key runs in the workspace and
+ * perm (int64[nnz]) receives the source position of every CSR entry, for
+ * fsb_gather_values.  Repeated (row, col) pairs keep their input order.
+ * Indices must lie inside the matrix (fsb_coo_inspect); nnz, n_rows and
+ * n_cols must be < 2^31.
+ * ------------------------------------------------------------------------ */
+FSB_API int fsb_coo_inspect(const void* row, int row_is_64, const void* col, int col_is_64, int64_t nnz,
+                      int64_t n_rows, int64_t n_cols, int64_t* d_out, void* stream);
+FSB_API int64_t fsb_coo_to_csr_workspace_bytes(int64_t nnz, int64_t n_rows, int64_t n_cols);
+FSB_API int fsb_coo_to_csr(const void* row, int row_is_64, const void* col, int col_is_64, int64_t nnz,
+                      int64_t n_rows, int64_t n_cols, int sorted, void* workspace, int64_t workspace_bytes,
+                      int32_t* out_col, int64_t* out_ptr, int64_t* perm, void* stream);
+
+/* ------------------------------------------------------------------------
  * CSR SpMV  y = A x.
  *
  * A launch plan splits the matrix into work units of one warp each:

@@ -25,6 +25,11 @@
  *      row-length bucket in ascending row order (torch.nonzero on each mask).
  *  oracle_spmv_plan       the native SpMV unit plan of this package (segments
  *      and work units), restated sequentially for bit-exact comparison.
+ *  oracle_coo_to_csr      sparse_operations/spmv_csr.py:948-984
+ *      (coo_to_csr_for_spmv): entries ordered by the key row * n_cols + col
+ *      (argsort), row pointers from bincount + cumsum.  Written as two stable
+ *      counting sorts (by column, then by row), so repeated (row, col) pairs
+ *      keep their input order.
  *
  * Index layout: indptr int64, column indices int32 (the Python wrapper
  * converts other layouts).  OpenMP parallelises over rows where rows are
@@ -195,6 +200,32 @@ void oracle_transpose(int64_t m, int64_t n, const int64_t* ptr, const int32_t* i
     }
   }
   free(cursor);
+}
+
+/* ---- COO -> CSR (stable order by (row, col)) ------------------------- */
+void oracle_coo_to_csr(int64_t m, int64_t n, int64_t nnz, const int64_t* row, const int64_t* col, int64_t* ptr,
+                       int32_t* idx, int64_t* perm) {
+  int64_t* tmp = (int64_t*)malloc(sizeof(int64_t) * (size_t)(nnz > 0 ? nnz : 1));
+  int64_t* cur = (int64_t*)calloc((size_t)(n + 1), sizeof(int64_t));
+  /* pass 1: stable counting sort of the positions by column */
+  for (int64_t k = 0; k < nnz; ++k) cur[col[k] + 1] += 1;
+  for (int64_t c = 0; c < n; ++c) cur[c + 1] += cur[c];
+  for (int64_t k = 0; k < nnz; ++k) tmp[cur[col[k]]++] = k;
+  free(cur);
+  /* pass 2: stable counting sort of that order by row; ptr = bincount + cumsum */
+  memset(ptr, 0, sizeof(int64_t) * (size_t)(m + 1));
+  for (int64_t k = 0; k < nnz; ++k) ptr[row[k] + 1] += 1;
+  for (int64_t r = 0; r < m; ++r) ptr[r + 1] += ptr[r];
+  int64_t* rc = (int64_t*)malloc(sizeof(int64_t) * (size_t)(m > 0 ? m : 1));
+  for (int64_t r = 0; r < m; ++r) rc[r] = ptr[r];
+  for (int64_t j = 0; j < nnz; ++j) {
+    const int64_t k = tmp[j];
+    const int64_t dst = rc[row[k]]++;
+    perm[dst] = k;
+    idx[dst] = (int32_t)col[k];
+  }
+  free(rc);
+  free(tmp);
 }
 
 /* ---- stable bucketing ------------------------------------------------- */

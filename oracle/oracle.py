@@ -33,6 +33,7 @@ _SIGS = {
     "oracle_spmm_f32_acc64": (None, [_i64, _i64, _p, _p, _p, _p, _p, _int]),
     "oracle_sddmm_dot2": (None, [_i64, _i64, _p, _p, _p, _p, _p, _dbl, _dbl, _p, _int]),
     "oracle_transpose": (None, [_i64, _i64, _p, _p, _p, _p, _p]),
+    "oracle_coo_to_csr": (None, [_i64, _i64, _i64, _p, _p, _p, _p, _p]),
     "oracle_bucketize": (None, [_i64, _p, _p, _int, _p, _p]),
     "oracle_spmv_plan": (None, [_i64, _p, _i64, _i64, _p, _p, _p, _p]),
 }
@@ -162,6 +163,18 @@ def transpose(indptr, indices, n_cols):
     perm = np.empty(nnz, dtype=np.int64)
     lib().oracle_transpose(m, int(n_cols), _ptr(ptr), _ptr(idx), _ptr(t_ptr), _ptr(t_idx), _ptr(perm))
     return t_ptr, t_idx, perm
+
+
+def coo_to_csr(row, col, n_rows, n_cols):
+    """COO pattern -> CSR: (indptr int64, indices int32, perm int64), stable in (row, col) order."""
+    r = _a(row, np.int64)
+    c = _a(col, np.int64)
+    nnz = r.size
+    ptr = np.empty(int(n_rows) + 1, dtype=np.int64)
+    idx = np.empty(nnz, dtype=np.int32)
+    perm = np.empty(nnz, dtype=np.int64)
+    lib().oracle_coo_to_csr(int(n_rows), int(n_cols), nnz, _ptr(r), _ptr(c), _ptr(ptr), _ptr(idx), _ptr(perm))
+    return ptr, idx, perm
 
 
 def bucketize(indptr, upper_bounds):

@@ -202,6 +202,29 @@ def sddmm_cases(dm, out):
             out[f"{tag}_{dname}_out"] = res.numpy()
 
 
+def coo_cases(m, out):
+    """coo_to_csr_for_spmv (spmv_csr.py:957-984) on distinct (row, col) pairs in
+    shuffled, sorted and empty-row layouts; int32 and int64 index inputs."""
+    rng = np.random.default_rng(21)
+    cases = [("shuf", 40, 33, 300, True, torch.int64), ("sorted", 25, 50, 200, False, torch.int64),
+             ("i32", 64, 17, 400, True, torch.int32), ("emptyrows", 500, 40, 120, True, torch.int64)]
+    for tag, nr, nc, nnz, shuffle, idt in cases:
+        keys = np.sort(rng.choice(nr * nc, size=nnz, replace=False))
+        if shuffle:
+            keys = rng.permutation(keys)
+        row = torch.from_numpy(keys // nc).to(idt)
+        col = torch.from_numpy(keys % nc).to(idt)
+        data = torch.from_numpy(rng.standard_normal(nnz)).to(torch.float32)
+        d_s, idx, ptr = m.coo_to_csr_for_spmv(data, row, col, (nr, nc))
+        out[f"coo_{tag}_shape"] = np.array([nr, nc], dtype=np.int64)
+        out[f"coo_{tag}_row"] = row.numpy()
+        out[f"coo_{tag}_col"] = col.numpy()
+        out[f"coo_{tag}_data"] = data.numpy()
+        out[f"coo_{tag}_data_s"] = np_of(d_s)
+        out[f"coo_{tag}_indices"] = idx.numpy()
+        out[f"coo_{tag}_indptr"] = ptr.numpy()
+
+
 def main():
     src = sys.argv[1] if len(sys.argv) > 1 else None
     if not src or not os.path.isdir(src):
@@ -217,6 +240,7 @@ def main():
         "golden_config1.npz": lambda o: config1_case(m, o),
         "golden_spmm.npz": lambda o: spmm_cases(sm, o),
         "golden_sddmm.npz": lambda o: sddmm_cases(dm, o),
+        "golden_coo.npz": lambda o: coo_cases(m, o),
     }
     only = set(sys.argv[2:])
     for fname, fn in groups.items():

@@ -31,7 +31,8 @@ def test_registry_shape_ids_and_interfaces():
     for snippet in ("description: |", "for:", "labels:", "kind:", "stages:"):
         assert snippet in text
     ids = re.findall(r"^  - id: ([a-z0-9_]+)$", text, flags=re.MULTILINE)
-    assert ids == ["spmv_csr", "spmm_csr", "spmm_csr_opt", "spmm_csr_opt_alg1", "spmm_csr_opt_alg2", "sddmm_csr"]
+    assert ids == ["spmv_csr", "spmm_csr", "spmm_csr_opt", "spmm_csr_opt_alg1", "spmm_csr_opt_alg2", "sddmm_csr",
+                   "spmv_coo_tocsr"]
     names = set(re.findall(r"^      - ([A-Za-z_][A-Za-z0-9_]*)$", text, flags=re.MULTILINE)) - IGNORED
     assert names and names <= set(fs.__all__)
 
@@ -72,6 +73,12 @@ SIGNATURES = {
                              ("shape", None), ("alpha", 1.0), ("beta", 0.0), ("prepared", None), ("out", None),
                              ("return_time", False), ("return_meta", False), ("allow_fallback", False)],
     "prepare_sddmm_csr": [("indices", E), ("indptr", E), ("shape", E), ("k_hint", 64)],
+    # spmv_csr.py:987-995, :1020-1033
+    "prepare_spmv_coo_tocsr": [("data", E), ("row", E), ("col", E), ("shape", E), ("block_nnz", 256),
+                               ("max_segments", None), ("assume_sorted", False)],
+    "flagsparse_spmv_coo_tocsr": [("data", None), ("row", None), ("col", None), ("x", None), ("shape", None),
+                                  ("block_nnz", 256), ("max_segments", None), ("out", None), ("return_time", False),
+                                  ("use_opt", True), ("prepared", None), ("assume_sorted", False)],
 }
 OPT = [("data", None), ("indices", None), ("indptr", None), ("B", None), ("shape", None), ("prepared", None),
        ("out", None), ("return_time", False), ("return_meta", False)]
