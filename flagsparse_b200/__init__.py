@@ -2,8 +2,8 @@
 
 Same public names and lazy export map as FlagSparse ``__init__.py``
 (``__all__`` ``:19-154``, ``_OPS_EXPORTS`` ``:156-272``, ``__getattr__``
-``:297-306``), restricted to the CSR SpMV / SpMM / SDDMM operators (and the COO-to-CSR
-SpMV on-ramp) this package implements.  ``import flagsparse_b200 as flagsparse`` is the switch.
+``:297-306``), restricted to the CSR SpMV / SpMM / SDDMM operators (with the COO-to-CSR
+SpMV on-ramp and the BSR SpMV) this package implements.  ``import flagsparse_b200 as flagsparse`` is the switch.
 """
 
 __version__ = "1.0.0"
@@ -18,6 +18,7 @@ _OPS_EXPORTS = {
     "SpmmCsrAlgorithmUnavailable",
     "prepare_spmv_csr",
     "prepare_spmv_coo_tocsr",
+    "prepare_spmv_bsr",
     "prepare_spmm_csr_route",
     "prepare_spmm_csr_opt",
     "prepare_spmm_csr_opt_alg1",
@@ -27,6 +28,7 @@ _OPS_EXPORTS = {
     "prepare_sddmm_csr",
     "flagsparse_spmv_csr",
     "flagsparse_spmv_coo_tocsr",
+    "flagsparse_spmv_bsr",
     "flagsparse_spmm_csr",
     "flagsparse_spmm_csr_run",
     "flagsparse_spmm_csr_opt",

@@ -83,6 +83,10 @@ _SIGNATURES = {
          _c_ptr, _c_int, _c_ptr, _c_int, _c_ptr, _c_ptr],
     ),
     "fsb_gather_values": (_c_int, [_c_int, _c_ptr, _c_ptr, _c_i64, _c_int, _c_ptr, _c_ptr]),
+    "fsb_bsr_spmv": (
+        _c_int, [_c_int, _c_ptr, _c_ptr, _c_int, _c_ptr, _c_int, _c_i64, _c_i64, _c_int, _c_ptr, _c_ptr, _c_ptr]
+    ),
+    "fsb_bsr_transpose_values": (_c_int, [_c_int, _c_ptr, _c_ptr, _c_i64, _c_int, _c_int, _c_ptr, _c_ptr]),
     "fsb_coo_inspect": (_c_int, [_c_ptr, _c_int, _c_ptr, _c_int, _c_i64, _c_i64, _c_i64, _c_ptr, _c_ptr]),
     "fsb_coo_to_csr_workspace_bytes": (_c_i64, [_c_i64, _c_i64, _c_i64]),
     "fsb_coo_to_csr": (

@@ -42,6 +42,7 @@ from .spmm_csr_opt_alg2 import (
     prepare_spmm_csr_opt_alg2,
     prepare_spmm_csr_opt_alg2_preprocess,
 )
+from .spmv_bsr import PreparedBsrSpmv, flagsparse_spmv_bsr, prepare_spmv_bsr
 from .spmv_csr import (
     PreparedCsrSpmv,
     flagsparse_spmv_coo_tocsr,
@@ -61,6 +62,7 @@ __all__ = [
     "PreparedCsrSpmmOpt",
     "PreparedCsrSpmmOptAlg2",
     "PreparedCsrSpmmRoute",
+    "PreparedBsrSpmv",
     "PreparedCsrSpmv",
     "SDDMMPrepared",
     "SpmmCsrAlgorithm",
@@ -75,6 +77,7 @@ __all__ = [
     "flagsparse_spmm_csr_opt_alg2",
     "flagsparse_spmm_csr_opt_alg2_preprocess",
     "flagsparse_spmm_csr_run",
+    "flagsparse_spmv_bsr",
     "flagsparse_spmv_coo_tocsr",
     "flagsparse_spmv_csr",
     "list_spmm_csr_algorithms",
@@ -87,6 +90,7 @@ __all__ = [
     "prepare_spmm_csr_opt_alg2",
     "prepare_spmm_csr_opt_alg2_preprocess",
     "prepare_spmm_csr_route",
+    "prepare_spmv_bsr",
     "prepare_spmv_coo_tocsr",
     "prepare_spmv_csr",
     "resolve_spmm_csr_algorithm",

@@ -128,6 +128,23 @@ FSB_API int fsb_coo_to_csr(const void* row, int row_is_64, const void* col, int 
                       int32_t* out_col, int64_t* out_ptr, int64_t* perm, void* stream);
 
 /* ------------------------------------------------------------------------
+ * BSR SpMV  y = A x, any block dimension bd (replaces the BSR SpMV kernels of
+ * sparse_operations/spmv_bsr.py:183-446).  blocks: [nnzb][bd][bd] row-major;
+ * indices: block columns; indptr: [n_block_rows + 1] block row pointers.  x
+ * has the padded length n_block_cols * bd, y receives all
+ * n_block_rows * bd padded rows (empty block rows give 0).  Compensated
+ * sums in block order: deterministic.  dtype: any of the six value types.
+ * A^T x runs on the transposed matrix: fsb_csr_transpose of the block
+ * pattern (n_cols = n_block_cols) gives its indices, row pointers and perm;
+ * fsb_bsr_transpose_values gives its blocks (conjugated when conj != 0).
+ * ------------------------------------------------------------------------ */
+FSB_API int fsb_bsr_spmv(int dtype, const void* blocks, const void* indices, int idx_is_64, const void* indptr,
+                      int ptr_is_64, int64_t n_block_rows, int64_t n_block_cols, int block_dim, const void* x,
+                      void* y, void* stream);
+FSB_API int fsb_bsr_transpose_values(int dtype, const void* src, const int64_t* perm, int64_t nnzb, int block_dim,
+                      int conj, void* dst, void* stream);
+
+/* ------------------------------------------------------------------------
  * CSR SpMV  y = A x.
  *
  * A launch plan splits the matrix into work units of one warp each:

@@ -177,6 +177,34 @@ def coo_to_csr(row, col, n_rows, n_cols):
     return ptr, idx, perm
 
 
+def bsr_to_csr(blocks, indices, indptr, block_dim):
+    """Expand a BSR matrix (blocks [nnzb, bd, bd] row-major) to CSR over the padded
+    shape: (indptr int64, indices int32, values), every stored block value kept.
+
+    Restates the index arithmetic of FlagSparse's BSR SpMV kernels
+    (sparse_operations/spmv_bsr.py:183-223: row = brow * bd + inner_row,
+    col = bcol * bd + inner_col); the SpMV itself then runs on the CSR oracle.
+    """
+    bd = int(block_dim)
+    bptr = _a(indptr, np.int64)
+    bcol = _a(indices, np.int64)
+    vals = np.asarray(blocks)
+    nbr = bptr.size - 1
+    lens = np.diff(bptr) * bd
+    ptr = np.zeros(nbr * bd + 1, dtype=np.int64)
+    ptr[1:] = np.cumsum(np.repeat(lens, bd))
+    idx = np.empty(int(ptr[-1]), dtype=np.int32)
+    out = np.empty(int(ptr[-1]), dtype=vals.dtype)
+    for br in range(nbr):
+        ks = np.arange(bptr[br], bptr[br + 1])
+        for r in range(bd):
+            row = br * bd + r
+            a, b = ptr[row], ptr[row + 1]
+            idx[a:b] = (bcol[ks][:, None] * bd + np.arange(bd)[None, :]).reshape(-1)
+            out[a:b] = vals[ks, r, :].reshape(-1)
+    return ptr, idx, out
+
+
 def bucketize(indptr, upper_bounds):
     """Row lists per length bucket (ascending rows); None = unbounded."""
     ptr = _a(indptr, np.int64)

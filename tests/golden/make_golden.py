@@ -225,12 +225,44 @@ def coo_cases(m, out):
         out[f"coo_{tag}_indptr"] = ptr.numpy()
 
 
+def bsr_cases(bm, out):
+    """_triton_spmv_bsr_kernel (spmv_bsr.py:603-671) for op non / trans / conj on small
+    BSR matrices with ragged logical shapes (padded rows and columns)."""
+    rng = np.random.default_rng(31)
+    for bd in (2, 3, 4, 16):
+        nbr, nbc = 9, 7
+        counts = rng.integers(0, 4, size=nbr)
+        counts[2] = 0
+        ptr = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        cols = np.concatenate([np.sort(rng.choice(nbc, size=c, replace=False)) for c in counts]).astype(np.int64)
+        nnzb = int(ptr[-1])
+        shape = (nbr * bd - 1, nbc * bd - 1)
+        out[f"bsr{bd}_indptr"] = ptr
+        out[f"bsr{bd}_indices"] = cols
+        out[f"bsr{bd}_shape"] = np.array(shape, dtype=np.int64)
+        for dname in ("float32", "float64", "complex64", "complex128"):
+            dt = TORCH_DT[dname]
+            blocks = rand_vec(rng, nnzb * bd * bd, dt).reshape(nnzb, bd, bd)
+            out[f"bsr{bd}_{dname}_blocks"] = np_of(blocks)
+            for op_name, op_code in (("non", 0), ("trans", 1), ("conj", 2)):
+                if op_name == "conj" and not dt.is_complex:
+                    continue
+                n_in = nbr * bd if op_code else nbc * bd
+                x = rand_vec(rng, n_in, dt)
+                p = bm.PreparedBsrSpmv(blocks, torch.from_numpy(cols), torch.from_numpy(ptr), shape, bd, nbr, nbc,
+                                       128, 1, int(counts.max()), op=op_code)
+                y = bm._triton_spmv_bsr_kernel(p, x, op_code)
+                out[f"bsr{bd}_{dname}_{op_name}_x"] = np_of(x)
+                out[f"bsr{bd}_{dname}_{op_name}_y"] = np_of(y)
+
+
 def main():
     src = sys.argv[1] if len(sys.argv) > 1 else None
     if not src or not os.path.isdir(src):
         raise SystemExit("usage: make_golden.py <FlagSparse>/src")
     sys.path.insert(0, src)
     from flagsparse.sparse_operations import sddmm_csr as dm
+    from flagsparse.sparse_operations import spmv_bsr as bm
     from flagsparse.sparse_operations import spmm_csr as sm
     from flagsparse.sparse_operations import spmv_csr as m
 
@@ -241,6 +273,7 @@ def main():
         "golden_spmm.npz": lambda o: spmm_cases(sm, o),
         "golden_sddmm.npz": lambda o: sddmm_cases(dm, o),
         "golden_coo.npz": lambda o: coo_cases(m, o),
+        "golden_bsr.npz": lambda o: bsr_cases(bm, o),
     }
     only = set(sys.argv[2:])
     for fname, fn in groups.items():

@@ -32,7 +32,7 @@ def test_registry_shape_ids_and_interfaces():
         assert snippet in text
     ids = re.findall(r"^  - id: ([a-z0-9_]+)$", text, flags=re.MULTILINE)
     assert ids == ["spmv_csr", "spmm_csr", "spmm_csr_opt", "spmm_csr_opt_alg1", "spmm_csr_opt_alg2", "sddmm_csr",
-                   "spmv_coo_tocsr"]
+                   "spmv_bsr", "spmv_coo_tocsr"]
     names = set(re.findall(r"^      - ([A-Za-z_][A-Za-z0-9_]*)$", text, flags=re.MULTILINE)) - IGNORED
     assert names and names <= set(fs.__all__)
 
@@ -73,6 +73,14 @@ SIGNATURES = {
                              ("shape", None), ("alpha", 1.0), ("beta", 0.0), ("prepared", None), ("out", None),
                              ("return_time", False), ("return_meta", False), ("allow_fallback", False)],
     "prepare_sddmm_csr": [("indices", E), ("indptr", E), ("shape", E), ("k_hint", 64)],
+    # spmv_bsr.py:895-912, :510-522
+    "flagsparse_spmv_bsr": [("data", None), ("indices", None), ("indptr", None), ("x", None), ("shape", None),
+                            ("block_dim", None), ("block_nnz", 128), ("max_segments", None), ("out", None),
+                            ("return_time", False), ("return_meta", False), ("prepared", None), ("transpose", None),
+                            ("op", None), ("use_opt", False), ("index_fallback_policy", "auto")],
+    "prepare_spmv_bsr": [("data", E), ("indices", E), ("indptr", E), ("shape", E), ("block_dim", E),
+                         ("block_nnz", 128), ("max_segments", None), ("transpose", False), ("op", None),
+                         ("use_opt", False), ("index_fallback_policy", "auto")],
     # spmv_csr.py:987-995, :1020-1033
     "prepare_spmv_coo_tocsr": [("data", E), ("row", E), ("col", E), ("shape", E), ("block_nnz", 256),
                                ("max_segments", None), ("assume_sorted", False)],
