@@ -248,6 +248,47 @@ class SpmvZipf:
         return oracle.spmv_f32_acc64(c["indptr"], c["indices"], c["data"], c["x"], nthreads=nthreads)
 
 
+class SpmvMtx(SpmvZipf):
+    """The SpMV step on a MatrixMarket matrix (fp32 values, int32 columns, x U[-1,1] seed 1)."""
+
+    dtype = "f32"
+
+    def __init__(self, device, path):
+        import torch
+
+        import flagsparse_b200 as fs
+        from flagsparse_b200 import mtx
+
+        data, indices, indptr, shape = mtx.mtx_to_csr_arrays(path)
+        self.name = "spmv_csr_mtx_" + os.path.splitext(os.path.basename(path))[0]
+        self.path = path
+        x = np.random.default_rng(1).uniform(-1.0, 1.0, shape[1]).astype(np.float32)
+        c = {"data": data.astype(np.float32), "indices": indices.astype(np.int32), "indptr": indptr, "x": x,
+             "shape": shape}
+        self.torch, self.fs, self.host, self.device = torch, fs, c, device
+        self.M, self.K = shape
+        self.nnz = int(indices.size)
+        self.data = torch.from_numpy(c["data"]).to(device)
+        self.indices = torch.from_numpy(c["indices"]).to(device)
+        self.indptr = torch.from_numpy(indptr).to(device)
+        self.x = torch.from_numpy(x).to(device)
+        self.prepared = fs.prepare_spmv_csr(self.data, self.indices, self.indptr, shape)
+        self.y = torch.empty(self.M, dtype=torch.float32, device=device)
+        self.x_host = torch.from_numpy(x).pin_memory()
+        self.y_host = torch.empty(self.M, dtype=torch.float32).pin_memory()
+        self.x_dev2 = torch.empty_like(self.x)
+        self.x_buf = [torch.empty_like(self.x) for _ in range(2)]
+        self.y_buf = [torch.empty_like(self.y) for _ in range(2)]
+        self.y_hosts = [torch.empty(self.M, dtype=torch.float32).pin_memory() for _ in range(2)]
+        self.s_in = torch.cuda.Stream(device=device)
+        self.s_out = torch.cuda.Stream(device=device)
+
+    def config(self):
+        return {"workload": self.name, "file": os.path.basename(self.path), "rows": self.M, "cols": self.K,
+                "nnz": self.nnz, "index_dtype": "int32", "indptr_dtype": "int64",
+                "l2": "flushed between timed steps (256 MiB write)"}
+
+
 def _event_median_ms(torch, fn, flush, reps=10, warm=3):
     """Median CUDA-event time of fn() with L2 flushed before every timed call."""
     for _ in range(warm):
@@ -669,6 +710,7 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the SpMM and autograd measurements")
     ap.add_argument("--case", default="spmv", choices=["spmv"] + sorted(CASES),
                     help="workload of the timed steps (default: the SpMV headline)")
+    ap.add_argument("--mtx", default=None, help="time the SpMV on this MatrixMarket file instead (fp32 values)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -689,8 +731,11 @@ def main():
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=device)
 
-    wl = SpmvZipf(device) if args.case == "spmv" else CASES[args.case](device)
-    headline = args.case == "spmv"
+    if args.mtx:
+        wl = SpmvMtx(device, args.mtx)
+    else:
+        wl = SpmvZipf(device) if args.case == "spmv" else CASES[args.case](device)
+    headline = args.case == "spmv" and not args.mtx
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
 
     def barrier():
@@ -786,6 +831,7 @@ def main():
             "vs_baseline": None,
             "dtype": wl.dtype,
             "data": ("synthetic (seeded Zipf(2) power-law CSR, values/x U[-1,1])" if headline
+                     else f"MatrixMarket file {os.path.basename(args.mtx)}, x U[-1,1]" if args.mtx
                      else "synthetic (seeded generators; see config.workload)"),
             "config": dict(wl.config(), parallelism=f"replicas{world}" if world > 1 else "single"),
             "e2e": {"value": round(e2e_val, 2), "unit": "GB/s", "h2d_bytes_per_step": h2d,

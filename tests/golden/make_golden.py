@@ -256,6 +256,25 @@ def bsr_cases(bm, out):
                 out[f"bsr{bd}_{dname}_{op_name}_y"] = np_of(y)
 
 
+def mtx_cases(tests_dir, out):
+    """FlagSparse's test loader load_mtx_to_csr_torch (tests/test_spmv.py:116-190)
+    on the .mtx fixtures in tests/golden/mtx, read on the CPU."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("fs_test_spmv", os.path.join(tests_dir, "test_spmv.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    mdir = os.path.join(HERE, "mtx")
+    for name in sorted(os.listdir(mdir)):
+        data, indices, indptr, shape = mod.load_mtx_to_csr_torch(os.path.join(mdir, name), dtype=torch.float64,
+                                                                 device=torch.device("cpu"))
+        tag = name[:-4]
+        out[f"mtx_{tag}_data"] = data.numpy()
+        out[f"mtx_{tag}_indices"] = indices.numpy()
+        out[f"mtx_{tag}_indptr"] = indptr.numpy()
+        out[f"mtx_{tag}_shape"] = np.array(shape, dtype=np.int64)
+
+
 def main():
     src = sys.argv[1] if len(sys.argv) > 1 else None
     if not src or not os.path.isdir(src):
@@ -274,6 +293,7 @@ def main():
         "golden_sddmm.npz": lambda o: sddmm_cases(dm, o),
         "golden_coo.npz": lambda o: coo_cases(m, o),
         "golden_bsr.npz": lambda o: bsr_cases(bm, o),
+        "golden_mtx.npz": lambda o: mtx_cases(os.path.join(os.path.dirname(src), "tests"), o),
     }
     only = set(sys.argv[2:])
     for fname, fn in groups.items():
