@@ -328,7 +328,7 @@ def _rows_fp64(torch, c, vals64, dense64, rows, take, owner):
 
 
 def _max_rel(got, ref):
-    return float((got - ref).abs().max() / ref.abs().max().clamp_min(1e-300))
+    return float((got.detach() - ref).abs().max() / ref.abs().max().clamp_min(1e-300))
 
 
 class SpmmPowerLaw:
@@ -542,6 +542,56 @@ class Bsr16:
         return self.M * self.n * 2, self.M * self.n * 2
 
 
+class BsrSpmv:
+    """y = A x for the 16 x 16-block BSR pattern of Bsr16 (65,536 x 65,536 blocks, 8 per block
+    row, seed 2) with fp32 values and x U[-1,1]: FlagSparse's BSR SpMV dtype (spmv_bsr.py:23-28).
+
+    Bytes per step: nnzb*256*4 + nnzb*4 + (n_brows+1)*8 + 2 * M*4 (x and y once).
+    """
+
+    dtype = "f32"
+
+    def __init__(self, device):
+        import torch
+
+        import flagsparse_b200 as fs
+        from flagsparse_b200 import workloads
+
+        self.torch, self.fs = torch, fs
+        self.name = "bsr16_spmv_65536x65536_blocks_f32"
+        c = workloads.bsr16()
+        self.n_brows = c["block_shape"][0]
+        self.M = self.n_brows * 16
+        self.nnzb = int(c["indices"].size)
+        blocks = torch.from_numpy(c["blocks"]).to(device)
+        self.p = fs.prepare_spmv_bsr(blocks, torch.from_numpy(c["indices"]).to(device),
+                                     torch.from_numpy(c["indptr"]).to(device), (self.M, self.M), 16)
+        g = torch.Generator(device=device).manual_seed(2)
+        self.x = torch.rand(self.M, device=device, generator=g) * 2 - 1
+        self.y = torch.empty(self.M, device=device)
+        self.x_host = self.x.cpu().pin_memory()
+        self.y_host = torch.empty(self.M).pin_memory()
+        self.x_dev2 = torch.empty_like(self.x)
+
+    def config(self):
+        return {"workload": self.name, "block_rows": self.n_brows, "blocks_per_row": 8, "nnzb": self.nnzb,
+                "block_dim": 16, "seed": 2, "l2": "flushed between timed steps (256 MiB write)"}
+
+    def alg_bytes(self):
+        return self.nnzb * (256 * 4 + 4) + (self.n_brows + 1) * 8 + 2 * self.M * 4
+
+    def step(self):
+        self.fs.flagsparse_spmv_bsr(x=self.x, prepared=self.p, out=self.y)
+
+    def e2e_step(self):
+        self.x_dev2.copy_(self.x_host, non_blocking=True)
+        self.fs.flagsparse_spmv_bsr(x=self.x_dev2, prepared=self.p, out=self.y)
+        self.y_host.copy_(self.y, non_blocking=True)
+
+    def e2e_bytes(self):
+        return self.M * 4, self.M * 4
+
+
 class BatchedMix:
     """256 CSR matrices, row counts log-uniform in [1,000, 200,000]: even ids 5-point stencils,
     odd ids random with Poisson(24) rows; fp32, each with x and a 16-column B (seed 4).
@@ -613,6 +663,7 @@ class BatchedMix:
 CASES = {
     "batched_f32": lambda d: BatchedMix(d),
     "bsr16_bf16_N128": lambda d: Bsr16(d, 128),
+    "bsr_spmv_f32_bd16": lambda d: BsrSpmv(d),
     "spmm_f32_N64": lambda d: SpmmPowerLaw(d, "f32", 64),
     "spmm_f32_N128": lambda d: SpmmPowerLaw(d, "f32", 128),
     "spmm_bf16_N128": lambda d: SpmmPowerLaw(d, "bf16", 128),
@@ -683,6 +734,12 @@ def measure_extras(torch, device, flush, peak):
                                    "tflops": round(case.flops() / ms / 1e9, 1),
                                    "tensor_frac_of_measured_bf16": round(case.flops() / ms / 1e9 / bf16_peak, 4),
                                    "nnzb": case.nnzb, "bound": "hbm (12 flop/byte, far below the tensor ridge)"}
+    del case
+    case = BsrSpmv(device)
+    ms = _event_median_ms(torch, case.step, flush)
+    out["bsr_spmv_f32_bd16"] = {"ms": round(ms, 4), "gbs": round(case.alg_bytes() / ms / 1e6, 1),
+                                "hbm_frac": round(case.alg_bytes() / ms / 1e6 / peak, 3), "nnzb": case.nnzb,
+                                "bytes_model": "nnzb*(256*4+4)+(n_brows+1)*8+2*M*4"}
     return out
 
 
