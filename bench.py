@@ -639,9 +639,12 @@ class BatchedMix:
         b = self.b
         return {"workload": self.name, "matrices": b.count, "rows": b.n_rows, "nnz": b.nnz, "dense_cols": 16,
                 "seed": 4, "schedule": {"spmv": b.spmv_cfg, "spmm": b.spmm_cfg,
+                                        "fused": b.fused,
                                         "spmv_trials": self.tuning["spmv_trials"],
-                                        "spmm_trials": self.tuning["spmm_trials"]},
-                "launch": "one CUDA graph: SpMV + SpMM over the block-diagonal batch",
+                                        "spmm_trials": self.tuning["spmm_trials"],
+                                        "fused_trials": self.tuning.get("fused_trials", [])},
+                "launch": ("one CUDA graph holding one kernel: fused SpMM + SpMV over the block-diagonal batch"
+                           if b.fused else "one CUDA graph: SpMV + SpMM launches over the block-diagonal batch"),
                 "l2": "flushed between timed steps (256 MiB write, then a 50 us device spin that covers the host call)"}
 
     def alg_bytes(self):
@@ -664,7 +667,9 @@ class BatchedMix:
         return (b.n_cols + b.n_cols * 16) * 4, (b.n_rows + b.n_rows * 16) * 4
 
     def launches_per_step(self):
-        p = self.b._plans()[0]
+        if self.b.fused:
+            return 1
+        p = self.b._spmv_plan_get()
         return int(p.n_block_units > 0) + int(p.n_units > p.n_block_units) + 1
 
 
@@ -732,7 +737,9 @@ def measure_extras(torch, device, flush, peak):
                                      "gather_model_gbs": round((spmv_b + spmm_g) / ms / 1e6, 1),
                                      "matrices": case.b.count, "rows": case.b.n_rows, "nnz": case.b.nnz,
                                      "schedule": {"spmv": case.b.spmv_cfg, "spmm": case.b.spmm_cfg},
-                                     "launch": "one CUDA graph replay (SpMV + SpMM over all 256 matrices)"}
+                                     "launch": ("one CUDA graph replay of one fused SpMM + SpMV kernel over all 256 matrices"
+                                                if case.b.fused else
+                                                "one CUDA graph replay (SpMV + SpMM over all 256 matrices)")}
     del case
     case = Bsr16(device)
     ms = _event_median_ms(torch, case.step, flush)

@@ -37,6 +37,10 @@ constexpr int kSpmmWarps = 8;      // warps per block; one (unit, tile) per warp
 constexpr int kSpmmBatch = 128;    // nonzeros staged per batch
 constexpr int kSpmmMaxCap = 64;    // row blocks hold < 2*cap <= kSpmmBatch nonzeros
 constexpr int kSpmmAhead = 4;      // B slices loaded ahead of the multiply-adds
+// the same for a team's row in the narrow-row kernel: 8 for fp32 (measured
+// 2-6 % faster), 4 where the slices, sums or the fused y terms need the registers
+template <int DT>
+struct TeamAhead { static constexpr int value = (DT == FSB_F32) ? 8 : 4; };
 constexpr int kSpmmTileLanes = 32;
 
 template <int BYTES> struct RawT;
@@ -165,6 +169,48 @@ constexpr int spmm_warp_smem_bytes() {
 
 template <int DT>
 struct SpmmMinBlocks { static constexpr int value = (DT == FSB_C128) ? 2 : (DT == FSB_F64 || DT == FSB_C64) ? 3 : 4; };
+
+// Gather of x for the fused y sums: L2-only.
+template <typename T> __device__ __forceinline__ T ld_gather(const T* p) { return __ldcg(p); }
+template <> __device__ __forceinline__ __half ld_gather<__half>(const __half* p) {
+  return __ushort_as_half(__ldcg(reinterpret_cast<const unsigned short*>(p)));
+}
+template <> __device__ __forceinline__ __nv_bfloat16 ld_gather<__nv_bfloat16>(const __nv_bfloat16* p) {
+  return __ushort_as_bfloat16(__ldcg(reinterpret_cast<const unsigned short*>(p)));
+}
+__device__ __forceinline__ void put_y(__half& o, float v) { o = __float2half_rn(v); }
+__device__ __forceinline__ void put_y(__nv_bfloat16& o, float v) { o = __float2bfloat16_rn(v); }
+__device__ __forceinline__ void put_y(float& o, float v) { o = v; }
+__device__ __forceinline__ void put_y(double& o, double v) { o = v; }
+
+// y accumulator of the fused SpMM + SpMV.  For 2- and 4-byte values every
+// product is exact in fp64, so an fp64 sum is at least as accurate as Dot2 in
+// fp32 and costs one DFMA per term; fp64 values keep the Dot2 pair.  A
+// long-row partial takes the two real slots of scratch column n.
+template <typename R> struct YAcc;
+template <> struct YAcc<float> {
+  double s;
+  __device__ __forceinline__ void zero() { s = 0.0; }
+  __device__ __forceinline__ void add_prod(float a, float b) { s = __fma_rn(double(a), double(b), s); }
+  __device__ __forceinline__ void shfl_join(int m) { s = __dadd_rn(s, __shfl_xor_sync(0xffffffffu, s, m)); }
+  __device__ __forceinline__ void store(float* p) const { *reinterpret_cast<double*>(p) = s; }
+  __device__ __forceinline__ void add_stored(const float* p) {
+    s = __dadd_rn(s, __ldcg(reinterpret_cast<const double*>(p)));
+  }
+  __device__ __forceinline__ float value() const { return __double2float_rn(s); }
+};
+template <> struct YAcc<double> {
+  Comp<double> c;
+  __device__ __forceinline__ void zero() { c.zero(); }
+  __device__ __forceinline__ void add_prod(double a, double b) { c.add_prod(a, b); }
+  __device__ __forceinline__ void shfl_join(int m) {
+    const double oh = __shfl_xor_sync(0xffffffffu, c.hi, m), ol = __shfl_xor_sync(0xffffffffu, c.lo, m);
+    c.add_comp(oh, ol);
+  }
+  __device__ __forceinline__ void store(double* p) const { p[0] = c.hi; p[1] = c.lo; }
+  __device__ __forceinline__ void add_stored(const double* p) { c.add_comp(__ldcg(p), __ldcg(p + 1)); }
+  __device__ __forceinline__ double value() const { return c.value(); }
+};
 
 template <typename T> __device__ __forceinline__ T ld_once(const T* p) { return __ldcs(p); }
 template <> __device__ __forceinline__ __half ld_once<__half>(const __half* p) {
@@ -343,17 +389,21 @@ __device__ __forceinline__ void acc_shfl_add(SpmmAcc<DT, COMP, V>& a, int m) {
     }
 }
 
-template <int DT, bool COMP>
+template <int DT, bool COMP, bool FUSED>
 __global__ void __launch_bounds__(kSpmmWarps * 32, SpmmMinBlocks<DT>::value)
 k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __restrict__ col,
             const int64_t* __restrict__ ptr, const typename VT<DT>::Store* __restrict__ B, int64_t ldb, int64_t n,
             typename VT<DT>::Store* __restrict__ C, int64_t ldc, fsb_spmv_plan plan, int T, int64_t pstride,
-            int64_t cps) {
+            int64_t cps, const typename VT<DT>::Store* __restrict__ x, typename VT<DT>::Store* __restrict__ y) {
   using S = typename VT<DT>::Store;
   using R = typename VT<DT>::Real;
   constexpr int V = 16 / int(sizeof(S));
   using Acc = SpmmAcc<DT, COMP, V>;
   constexpr int kER = Acc::kNC * 2;
+  constexpr int kTA = FUSED ? 4 : TeamAhead<DT>::value;
+  // FUSED: the team's lanes also sum y = A x for its rows (item q * T + tl of
+  // each group of loads to lane tl), gathering x[col] beside the B row of the
+  // same nonzero.
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -391,21 +441,45 @@ k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __re
       for (int m = T; m < 32; m <<= 1) maxlen = max(maxlen, __shfl_xor_sync(0xffffffffu, maxlen, m));
       Acc acc;
       acc.zero();
-      for (int k = 0; k < maxlen; k += kSpmmAhead) {
-        S bv[kSpmmAhead][V];
+      YAcc<R> yacc;
+      yacc.zero();
+      for (int k = 0; k < maxlen; k += kTA) {
+        S bv[kTA][V];
+        S xv[kTA];
 #pragma unroll
-        for (int u = 0; u < kSpmmAhead; ++u) {
+        for (int u = 0; u < kTA; ++u) {
           const bool ok = k + u < len;
           load_slice<S, V>(B + int64_t(sh_c[ok ? b + k + u : 0]) * ldb + c0, ok ? nv : 0, bv[u]);
         }
+        if constexpr (FUSED) {
+          // item q * T + tl of this group goes to lane tl: every lane works at once
 #pragma unroll
-        for (int u = 0; u < kSpmmAhead; ++u)
+          for (int q = 0; q < kTA; ++q) {
+            const int u = q * T + tl;
+            if (q * T < kTA && u < kTA && k + u < len) xv[q] = ld_gather(x + sh_c[b + k + u]);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kTA; ++u)
           if (k + u < len) acc.add(sh_a[b + k + u], bv[u]);
+        if constexpr (FUSED) {
+#pragma unroll
+          for (int q = 0; q < kTA; ++q) {
+            const int u = q * T + tl;
+            if (q * T < kTA && u < kTA && k + u < len)
+              yacc.add_prod(to_real(sh_a[b + k + u]), to_real(xv[q]));
+          }
+        }
       }
       if (has && nv > 0) {
         S o[V];
         acc.result(o);
         store_slice(C + (int64_t(row) + i) * ldc + c0, nv, o);
+      }
+      if constexpr (FUSED) {
+        // join the y terms spread over the team's lanes
+        for (int m = 1; m < T; m <<= 1) yacc.shfl_join(m);
+        if (has && tl == 0) put_y(y[int64_t(row) + i], yacc.value());
       }
     }
     return;
@@ -415,6 +489,8 @@ k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __re
   const int32_t nch = __ldg(&ud->n_chunks), slot = __ldg(&ud->slot);
   Acc acc;
   acc.zero();
+  YAcc<R> yacc;
+  yacc.zero();
   for (int64_t b0 = s0; b0 < s1; b0 += kSpmmBatch) {
     const int cnt = static_cast<int>(s1 - b0 < kSpmmBatch ? s1 - b0 : int64_t(kSpmmBatch));
     __syncwarp();
@@ -425,30 +501,56 @@ k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __re
     __syncwarp();
     for (int k = 0; k < cnt; k += kSpmmAhead * G) {
       S bv[kSpmmAhead][V];
+      S xv[kSpmmAhead];
 #pragma unroll
       for (int u = 0; u < kSpmmAhead; ++u) {
         const int kk = k + u * G + team;
         load_slice<S, V>(B + int64_t(sh_c[kk < cnt ? kk : 0]) * ldb + c0, kk < cnt ? nv : 0, bv[u]);
+      }
+      if constexpr (FUSED) {
+        // the y terms of these kSpmmAhead * G items, one per lane in order
+#pragma unroll
+        for (int q = 0; q * 32 < kSpmmAhead * G; ++q) {
+          const int kk = k + q * 32 + lane;
+          if (q * 32 + lane < kSpmmAhead * G && kk < cnt) xv[q] = ld_gather(x + sh_c[kk]);
+        }
       }
 #pragma unroll
       for (int u = 0; u < kSpmmAhead; ++u) {
         const int kk = k + u * G + team;
         if (kk < cnt) acc.add(sh_a[kk], bv[u]);
       }
+      if constexpr (FUSED) {
+#pragma unroll
+        for (int q = 0; q * 32 < kSpmmAhead * G; ++q) {
+          const int kk = k + q * 32 + lane;
+          if (q * 32 + lane < kSpmmAhead * G && kk < cnt) yacc.add_prod(to_real(sh_a[kk]), to_real(xv[q]));
+        }
+      }
     }
   }
   for (int m = T; m < 32; m <<= 1) acc_shfl_add(acc, m);  // every team now holds the chunk's sum
+  if constexpr (FUSED) {
+    // every lane's y terms, joined over the warp in a fixed order
+    for (int m = 1; m < 32; m <<= 1) yacc.shfl_join(m);
+  }
   if (nch == 1) {
     if (team == 0 && nv > 0) {
       S o[V];
       acc.result(o);
       store_slice(C + int64_t(row) * ldc + c0, nv, o);
     }
+    if constexpr (FUSED)
+      if (lane == 0) put_y(y[row], yacc.value());
     return;
   }
   R* part = static_cast<R*>(plan.partials);
   const int64_t first = int64_t(slot) + (tag + 1);
   if (team == 0) acc.store_partial(part + (int64_t(slot) * pstride + c0) * kER);
+  if constexpr (FUSED) {
+    // y's partial sits in the slot's column n (n < pstride for the fused path)
+    if (lane == 0) yacc.store(part + (int64_t(slot) * pstride + n) * kER);
+  }
   __threadfence();
   __syncwarp();
   int ticket = 0;
@@ -465,6 +567,14 @@ k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __re
     S o[V];
     fin.result(o);
     store_slice(C + int64_t(row) * ldc + c0, nv, o);
+  }
+  if constexpr (FUSED) {
+    if (lane == 0) {
+      YAcc<R> fy;
+      fy.zero();
+      for (int c = 0; c < nch; ++c) fy.add_stored(part + ((first + c) * pstride + n) * kER);
+      put_y(y[row], fy.value());
+    }
   }
   if (lane == 0) plan.counters[first * cps] = 0;  // ready for the next call
 }
@@ -519,17 +629,41 @@ int spmm_pick_v(const void* B, int64_t ldb, const void* C, int64_t ldc, int64_t 
   return v;
 }
 
-template <int DT, bool COMP>
+template <int DT, bool COMP, bool FUSED = false>
 int spmm_launch_team(const void* data, const int32_t* idx, const int64_t* ptr, const void* B, int64_t ldb, int64_t n,
-                     void* C, int64_t ldc, const fsb_spmv_plan& plan, int T, cudaStream_t st) {
+                     void* C, int64_t ldc, const fsb_spmv_plan& plan, int T, cudaStream_t st,
+                     const void* x = nullptr, void* y = nullptr) {
   using S = typename VT<DT>::Store;
   const int64_t blocks = ceil_div(plan.n_units, kSpmmWarps);
   const size_t smem = size_t(spmm_warp_smem_bytes<S>()) * kSpmmWarps;
-  k_spmm_team<DT, COMP><<<(unsigned)blocks, kSpmmWarps * 32, smem, st>>>(
+  k_spmm_team<DT, COMP, FUSED><<<(unsigned)blocks, kSpmmWarps * 32, smem, st>>>(
       static_cast<const S*>(data), idx, ptr, static_cast<const S*>(B), ldb, n, static_cast<S*>(C), ldc, plan, T,
-      spmm_pstride(n), spmm_cps(n));
+      spmm_pstride(n), spmm_cps(n), static_cast<const S*>(x), static_cast<S*>(y));
   FSB_LAUNCH_CHECK();
   return FSB_OK;
+}
+
+// C = A B and y = A x in one launch: the team kernel with the fused y sums.
+// Real types, narrow aligned rows (the team conditions) and n < the slot
+// stride, so that y's long-row partial has a column of its own.
+template <int DT>
+int spmm_spmv_fused(const void* data, const int32_t* idx, const int64_t* ptr, const void* B, int64_t ldb, int64_t n,
+                    void* C, int64_t ldc, const void* x, void* y, const fsb_spmv_plan& plan, cudaStream_t st) {
+  using S = typename VT<DT>::Store;
+  constexpr int kVmax = 16 / int(sizeof(S));
+  if constexpr (VT<DT>::kComplex) {
+    return FSB_ERR_UNSUPPORTED;
+  } else {
+    if (!(n * int64_t(sizeof(S)) <= 256 && n % kVmax == 0 && ldb % kVmax == 0 && ldc % kVmax == 0 &&
+          reinterpret_cast<uintptr_t>(B) % 16 == 0 && reinterpret_cast<uintptr_t>(C) % 16 == 0 &&
+          n < spmm_pstride(n)))
+      return FSB_ERR_UNSUPPORTED;
+    int T = 1;
+    while (int64_t(T) * kVmax < n) T *= 2;
+    if (plan.flags & FSB_SPMM_COMPENSATED)
+      return spmm_launch_team<DT, true, true>(data, idx, ptr, B, ldb, n, C, ldc, plan, T, st, x, y);
+    return spmm_launch_team<DT, false, true>(data, idx, ptr, B, ldb, n, C, ldc, plan, T, st, x, y);
+  }
 }
 
 template <int DT, bool COMP>
@@ -601,6 +735,27 @@ int fsb_spmm_csr(int dtype, const void* data, const int32_t* indices, const int6
     case FSB_F64: return spmm_mode<FSB_F64>(data, indices, indptr, B, ldb, n, C, ldc, *plan, st);
     case FSB_C64: return spmm_mode<FSB_C64>(data, indices, indptr, B, ldb, n, C, ldc, *plan, st);
     case FSB_C128: return spmm_mode<FSB_C128>(data, indices, indptr, B, ldb, n, C, ldc, *plan, st);
+    default: return FSB_ERR_UNSUPPORTED;
+  }
+}
+
+int fsb_spmm_spmv_csr(int dtype, const void* data, const int32_t* indices, const int64_t* indptr, int64_t n_rows,
+                      int64_t n_cols, const void* B, int64_t ldb, int64_t n, void* C, int64_t ldc, const void* x,
+                      void* y, const fsb_spmv_plan* plan, void* stream) {
+  if (!plan || n_rows < 0 || n_cols < 0 || n < 1 || ldb < n || ldc < n || !x || !y) return FSB_ERR_INVALID_ARG;
+  if (n_rows == 0) return FSB_OK;
+  if (!indptr || !C || !plan->units || plan->n_units < 1 || plan->cap < 1 || plan->cap > kSpmmMaxCap ||
+      plan->chunk_nnz < kSpmmBatch || plan->chunk_nnz % kSpmmBatch != 0 || plan->n_slots < 0 ||
+      (plan->n_slots > 0 && (!plan->partials || !plan->counters)))
+    return FSB_ERR_INVALID_ARG;
+  if (n_cols > 0 && !B) return FSB_ERR_INVALID_ARG;
+  if (plan->n_units >= INT32_MAX) return FSB_ERR_UNSUPPORTED;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  switch (dtype) {
+    case FSB_F16: return spmm_spmv_fused<FSB_F16>(data, indices, indptr, B, ldb, n, C, ldc, x, y, *plan, st);
+    case FSB_BF16: return spmm_spmv_fused<FSB_BF16>(data, indices, indptr, B, ldb, n, C, ldc, x, y, *plan, st);
+    case FSB_F32: return spmm_spmv_fused<FSB_F32>(data, indices, indptr, B, ldb, n, C, ldc, x, y, *plan, st);
+    case FSB_F64: return spmm_spmv_fused<FSB_F64>(data, indices, indptr, B, ldb, n, C, ldc, x, y, *plan, st);
     default: return FSB_ERR_UNSUPPORTED;
   }
 }

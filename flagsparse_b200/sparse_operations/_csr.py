@@ -282,6 +282,25 @@ class SpmmPlan:
         return all(int(c.abs().sum().item()) == 0 for _, c, _ in self._scratch.values())
 
 
+def spmm_spmv(data, indices, indptr, n_rows, n_cols, B, plan, out, x, y, compensated=False):
+    """out = A @ B and y = A @ x in one launch through fsb_spmm_spmv_csr.
+
+    Returns False (nothing launched) when the fused kernel does not apply
+    (complex values, wide or misaligned dense rows, N a multiple of 256).
+    """
+    n = int(B.shape[1])
+    rc = nat.lib().fsb_spmm_spmv_csr(
+        nat.dtype_code(data.dtype), nat.ptr(data), nat.ptr(indices), nat.ptr(indptr), int(n_rows), int(n_cols),
+        nat.ptr(B), int(B.stride(0)) if B.shape[0] > 1 else max(n, 1), n, nat.ptr(out),
+        int(out.stride(0)) if out.shape[0] > 1 else max(n, 1), nat.ptr(x), nat.ptr(y),
+        plan.struct_for(n, compensated), nat.stream_of(out.device),
+    )
+    if rc == nat.FSB_ERR_UNSUPPORTED:
+        return False
+    nat.check(rc, "fsb_spmm_spmv_csr")
+    return True
+
+
 def spmm(data, indices, indptr, n_rows, n_cols, B, plan, out, compensated=False):
     """out[:n_rows, :N] = A @ B through fsb_spmm_csr.
 

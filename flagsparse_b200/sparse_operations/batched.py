@@ -6,15 +6,21 @@ and one SpMM over the combined matrix then compute every y_i = A_i x_i and
 C_i = A_i B_i, because the unit plan cuts work across matrix boundaries like
 any other row boundary: large and small matrices share the same warps.
 
+A step is either the SpMV and the SpMM launches, or -- for real values with a
+narrow B (N * sizeof(value) <= 256 bytes) -- ONE kernel: the narrow-row SpMM
+kernel whose lanes also sum y = A x from x[col] gathered beside B's row
+(``fsb_spmm_spmv_csr``), which reads the matrix once for both products.  The
+autotuner times both and keeps the faster; untuned, the step is unfused.
+
 Inputs and outputs live in static device buffers (``x``, ``B``, ``y``, ``C``)
-with one view per matrix; ``capture()`` records both launches in a CUDA graph
-and ``run()`` replays it, so a step is a single host launch.
+with one view per matrix; ``capture()`` records the step in a CUDA graph and
+``run()`` replays it, so a step is a single host launch.
 
 ``tune()`` is the schedule autotuner: it times candidate plan parameters (the
 row-block window ``cap`` and the long-row chunk of the SpMV and the SpMM
-plans) on this batch and keeps the fastest; results are cached per batch
-signature (dtype, width, row-length histogram) in memory and, when a path is
-given, in a JSON file.
+plans) and the fused step on this batch and keeps the fastest schedule;
+results are cached per batch signature (dtype, width, row-length histogram)
+in memory and, when a path is given, in a JSON file.
 """
 
 import json
@@ -88,6 +94,7 @@ class BatchedCsr:
         self._spmv_plan = self._spmm_plan = None
         self._graph = None
         self.tuning = None
+        self.fused = False  # the one-kernel step, when the autotuner picks it
 
     # ------------------------------------------------------------ views
     def x_view(self, i):
@@ -103,14 +110,20 @@ class BatchedCsr:
         return self.C[self.row_off[i]:self.row_off[i + 1]]
 
     # ------------------------------------------------------------ launches
-    def _plans(self):
+    def _spmv_plan_get(self):
         if self._spmv_plan is None:
             self._spmv_plan = _csr.NativeSpmvPlan(self.indptr, self.n_rows, self.dtype, cap=self.spmv_cfg["cap"],
                                                   chunk_nnz=self.spmv_cfg["chunk"])
+        return self._spmv_plan
+
+    def _spmm_plan_get(self):
         if self._spmm_plan is None:
             self._spmm_plan = _csr.SpmmPlan(self.indptr, self.n_rows, self.dtype, cap=self.spmm_cfg["cap"],
                                             chunk_nnz=self.spmm_cfg["chunk"])
-        return self._spmv_plan, self._spmm_plan
+        return self._spmm_plan
+
+    def _plans(self):
+        return self._spmv_plan_get(), self._spmm_plan_get()
 
     def _launch_spmv(self, plan):
         nat.check(
@@ -123,11 +136,19 @@ class BatchedCsr:
     def _launch_spmm(self, plan):
         _csr.spmm(self.data, self.indices, self.indptr, self.n_rows, self.n_cols, self.B, plan, self.C)
 
+    def _launch_fused(self, plan):
+        return _csr.spmm_spmv(self.data, self.indices, self.indptr, self.n_rows, self.n_cols, self.B, plan, self.C,
+                              self.x, self.y)
+
     def step(self):
-        """One SpMV and one SpMM over the whole batch (two launches, no graph)."""
-        spmv_plan, spmm_plan = self._plans()
-        self._launch_spmv(spmv_plan)
-        self._launch_spmm(spmm_plan)
+        """y = A x and C = A B over the whole batch (no graph): the fused launch when
+        selected and applicable, else the SpMV and the SpMM launches."""
+        if self.fused:
+            if self._launch_fused(self._spmm_plan_get()):
+                return
+            self.fused = False
+        self._launch_spmv(self._spmv_plan_get())
+        self._launch_spmm(self._spmm_plan_get())
 
     # ------------------------------------------------------------ autotuner
     def _time(self, fn, reps=5):
@@ -151,12 +172,13 @@ class BatchedCsr:
                 cached = json.load(f).get(sig)
         if cached is not None:
             self.spmv_cfg, self.spmm_cfg = dict(cached["spmv"]), dict(cached["spmm"])
+            self.fused = bool(cached.get("fused", False))
             self._spmv_plan = self._spmm_plan = None
             self._graph = None
             self.tuning = dict(cached, source="cache")
             return self.tuning
-        report = {"signature": sig, "spmv_trials": [], "spmm_trials": []}
-        best_v = best_m = None
+        report = {"signature": sig, "spmv_trials": [], "spmm_trials": [], "fused_trials": []}
+        best_v = best_m = best_f = None
         max_cap = int(nat.lib().fsb_spmv_default_cap(nat.dtype_code(self.dtype)))
         for frac in SPMV_CANDIDATES:
             cfg = {"cap": max_cap // frac["cap"], "chunk": frac["chunk"]}
@@ -165,16 +187,25 @@ class BatchedCsr:
             report["spmv_trials"].append(dict(cfg, ms=round(ms, 5)))
             if best_v is None or ms < best_v[1]:
                 best_v = (cfg, ms)
+        fusable = self._launch_fused(self._spmm_plan_get())
         for cfg in SPMM_CANDIDATES:
             plan = _csr.SpmmPlan(self.indptr, self.n_rows, self.dtype, cap=cfg["cap"], chunk_nnz=cfg["chunk"])
             ms = self._time(lambda: self._launch_spmm(plan))
             report["spmm_trials"].append(dict(cfg, ms=round(ms, 5)))
             if best_m is None or ms < best_m[1]:
                 best_m = (cfg, ms)
-        self.spmv_cfg, self.spmm_cfg = dict(best_v[0]), dict(best_m[0])
+            if fusable:
+                ms = self._time(lambda: self._launch_fused(plan))
+                report["fused_trials"].append(dict(cfg, ms=round(ms, 5)))
+                if best_f is None or ms < best_f[1]:
+                    best_f = (cfg, ms)
+        self.fused = best_f is not None and best_f[1] < best_v[1] + best_m[1]
+        self.spmv_cfg = dict(best_v[0])
+        self.spmm_cfg = dict(best_f[0] if self.fused else best_m[0])
+        fused = self.fused
         self._spmv_plan = self._spmm_plan = None
         self._graph = None
-        report.update(spmv=self.spmv_cfg, spmm=self.spmm_cfg)
+        report.update(spmv=self.spmv_cfg, spmm=self.spmm_cfg, fused=bool(fused))
         _TUNE_CACHE[sig] = report
         if cache_path:
             data = {}
@@ -189,9 +220,8 @@ class BatchedCsr:
 
     # ------------------------------------------------------------ graph
     def capture(self):
-        """Record the batch step (SpMV + SpMM launches) in a CUDA graph on a side stream."""
-        self._plans()
-        self.step()  # scratch for this width exists before capture; kernels are loaded
+        """Record the batch step in a CUDA graph on a side stream."""
+        self.step()  # decides fused / unfused; scratch for this width exists before capture
         torch.cuda.synchronize(self.device)
         stream = torch.cuda.Stream(device=self.device)
         graph = torch.cuda.CUDAGraph()

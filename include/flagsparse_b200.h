@@ -285,6 +285,18 @@ FSB_API int fsb_spmm_csr(int dtype, const void* data, const int32_t* indices, co
                  int64_t n_rows, int64_t n_cols, const void* B, int64_t ldb, int64_t n,
                  void* C, int64_t ldc, const fsb_spmv_plan* plan, void* stream);
 
+/* C = A B and y = A x in one launch (one pass over A's values and columns):
+ * the narrow-row SpMM kernel whose team leaders also sum y, compensated, from
+ * x[col] gathered beside B's row.  Real dtypes only; needs n * sizeof(value)
+ * <= 256, n a multiple of 16 / sizeof(value), 16-byte aligned B and C with
+ * such leading dimensions, and n not a multiple of 256 (y's long-row partial
+ * takes column n of the slot scratch that fsb_spmm_scratch_layout sizes for
+ * n).  Returns FSB_ERR_UNSUPPORTED otherwise, with nothing launched; the
+ * caller then runs fsb_spmm_csr and fsb_spmv_csr.  plan as for fsb_spmm_csr. */
+FSB_API int fsb_spmm_spmv_csr(int dtype, const void* data, const int32_t* indices, const int64_t* indptr,
+                      int64_t n_rows, int64_t n_cols, const void* B, int64_t ldb, int64_t n, void* C, int64_t ldc,
+                      const void* x, void* y, const fsb_spmv_plan* plan, void* stream);
+
 /* ------------------------------------------------------------------------
  * CSR SDDMM  out[p] = alpha * <x[row(p)], y[col(p)]> + beta * in[p].
  *

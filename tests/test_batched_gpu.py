@@ -68,10 +68,15 @@ def test_batched_autotuner_picks_and_caches(tmp_path):
     rep = b.tune(cache_path=path)
     assert rep["source"] == "measured"
     assert len(rep["spmv_trials"]) == len(bm.SPMV_CANDIDATES) and len(rep["spmm_trials"]) == len(bm.SPMM_CANDIDATES)
+    # fp32 with a 16-column B: the one-kernel step applies and is timed too
+    assert len(rep["fused_trials"]) == len(bm.SPMM_CANDIDATES)
     fastest_v = min(rep["spmv_trials"], key=lambda t: t["ms"])
     fastest_m = min(rep["spmm_trials"], key=lambda t: t["ms"])
+    fastest_f = min(rep["fused_trials"], key=lambda t: t["ms"])
+    assert rep["fused"] == (fastest_f["ms"] < fastest_v["ms"] + fastest_m["ms"]) == b.fused
+    best = fastest_f if b.fused else fastest_m
     assert b.spmv_cfg == {"cap": fastest_v["cap"], "chunk": fastest_v["chunk"]}
-    assert b.spmm_cfg == {"cap": fastest_m["cap"], "chunk": fastest_m["chunk"]}
+    assert b.spmm_cfg == {"cap": best["cap"], "chunk": best["chunk"]}
     b.run()
     torch.cuda.synchronize()
     _check_all(b, mats, "tuned")
@@ -96,6 +101,36 @@ def test_spmv_smaller_windows_match(cap):
     ref = oracle.spmv(c["indptr"], c["indices"], d, c["x"].astype(np.float64))
     scale = oracle.spmv_abs(c["indptr"], c["indices"], d, c["x"].astype(np.float64))
     assert_spmv_close(host(b.y).astype(np.float64), ref, scale, np.diff(c["indptr"]), "float32", f"cap {cap}")
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64, torch.complex64])
+@pytest.mark.parametrize("fused", [False, True])
+def test_batched_fused_and_unfused_steps_match_oracle(dtype, fused):
+    """Both step forms, graph-captured: the one-kernel step for real values (complex values
+    fall back to the SpMV and SpMM launches) and the two-launch step."""
+    mats, _ = _batch(count=6, seed=15)
+    dev_m = [(torch.from_numpy(m["data"]).cuda().to(dtype), torch.from_numpy(m["indices"]).cuda(),
+              torch.from_numpy(m["indptr"]).cuda(), m["shape"]) for m in mats]
+    b = fs.BatchedCsr(dev_m, n_dense=16)
+    b.fused = fused
+    g = torch.Generator(device="cuda").manual_seed(6)
+    b.x.copy_(torch.rand(b.x.shape, device="cuda", generator=g).to(dtype))
+    b.B.copy_(torch.rand(b.B.shape, device="cuda", generator=g).to(dtype))
+    b.run()
+    torch.cuda.synchronize()
+    assert b.fused is (fused and not dtype.is_complex)
+    dname = {torch.float32: "float32", torch.float64: "float64", torch.complex64: "complex64"}[dtype]
+    for i, m in enumerate(mats):
+        d = m["data"].astype(np.complex128 if dtype.is_complex else np.float64)
+        x = host(b.x_view(i)).astype(d.dtype)
+        B = host(b.B_view(i)).astype(d.dtype)
+        ref = oracle.spmv(m["indptr"], m["indices"], d, x)
+        scale = oracle.spmv_abs(m["indptr"], m["indices"], np.abs(d), np.abs(x))
+        assert_spmv_close(host(b.y_view(i)), ref, scale, np.diff(m["indptr"]), dname, f"y {i}")
+        C_ref = oracle.spmm(m["indptr"], m["indices"], d, B)
+        C_scale = oracle.spmm(m["indptr"], m["indices"], np.abs(d), np.abs(B))
+        lens = np.broadcast_to(np.diff(m["indptr"])[:, None], C_ref.shape)
+        assert_within(host(b.C_view(i)), C_ref, plain_error_bound(dname, C_ref, C_scale, lens), f"C {i}")
 
 
 def test_batched_validation():
