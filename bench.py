@@ -248,6 +248,36 @@ class SpmvZipf:
         return oracle.spmv_f32_acc64(c["indptr"], c["indices"], c["data"], c["x"], nthreads=nthreads)
 
 
+class SpmvZipf64(SpmvZipf):
+    """The headline matrix as the float64 drop-in: fp64 values, x and y (same pattern, seed 1)."""
+
+    name = "spmv_csr_zipf2_2Mx2M_f64"
+    dtype = "f64"
+
+    def __init__(self, device, seed=1):
+        super().__init__(device, seed)
+        torch = self.torch
+        self.data = self.data.double()
+        self.x = self.x.double()
+        self.prepared = self.fs.prepare_spmv_csr(self.data, self.indices, self.indptr, self.host["shape"])
+        self.y = torch.empty(self.M, dtype=torch.float64, device=device)
+        self.x_host = self.x.cpu().pin_memory()
+        self.y_host = torch.empty(self.M, dtype=torch.float64).pin_memory()
+        self.x_dev2 = torch.empty_like(self.x)
+        self.x_buf = [torch.empty_like(self.x) for _ in range(2)]
+        self.y_buf = [torch.empty_like(self.y) for _ in range(2)]
+        self.y_hosts = [torch.empty(self.M, dtype=torch.float64).pin_memory() for _ in range(2)]
+
+    def config(self):
+        return dict(super().config(), workload=self.name, value_dtype="float64")
+
+    def alg_bytes(self):
+        return self.nnz * (8 + 4) + (self.M + 1) * 8 + self.K * 8 + self.M * 8
+
+    def e2e_bytes(self):
+        return self.K * 8, self.M * 8
+
+
 class SpmvMtx(SpmvZipf):
     """The SpMV step on a MatrixMarket matrix (fp32 values, int32 columns, x U[-1,1] seed 1)."""
 
@@ -677,6 +707,7 @@ CASES = {
     "batched_f32": lambda d: BatchedMix(d),
     "bsr16_bf16_N128": lambda d: Bsr16(d, 128),
     "bsr_spmv_f32_bd16": lambda d: BsrSpmv(d),
+    "spmv_f64": lambda d: SpmvZipf64(d),
     "spmm_f32_N64": lambda d: SpmmPowerLaw(d, "f32", 64),
     "spmm_f32_N128": lambda d: SpmmPowerLaw(d, "f32", 128),
     "spmm_bf16_N128": lambda d: SpmmPowerLaw(d, "bf16", 128),
@@ -749,6 +780,12 @@ def measure_extras(torch, device, flush, peak):
                                    "tflops": round(case.flops() / ms / 1e9, 1),
                                    "tensor_frac_of_measured_bf16": round(case.flops() / ms / 1e9 / bf16_peak, 4),
                                    "nnzb": case.nnzb, "bound": "hbm (12 flop/byte, far below the tensor ridge)"}
+    del case
+    case = SpmvZipf64(device)
+    ms = _event_median_ms(torch, case.step, flush)
+    out["spmv_f64_zipf2M"] = {"ms": round(ms, 4), "gbs": round(case.alg_bytes() / ms / 1e6, 1),
+                              "hbm_frac": round(case.alg_bytes() / ms / 1e6 / peak, 3),
+                              "bytes_model": "nnz*(8+4)+(M+1)*8+K*8+M*8"}
     del case
     case = BsrSpmv(device)
     ms = _event_median_ms(torch, case.step, flush)
