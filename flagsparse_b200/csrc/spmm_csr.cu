@@ -88,6 +88,17 @@ __device__ __forceinline__ __nv_bfloat16 spmm_store(float v, __nv_bfloat16*) { r
 __device__ __forceinline__ float spmm_store(float v, float*) { return v; }
 __device__ __forceinline__ double spmm_store(double v, double*) { return v; }
 
+// c0 += a * b0, c1 += a * b1 in one packed fp32x2 FMA (sm_100a); each half is
+// rounded exactly as a scalar fma.rn, so results equal the scalar loop's.
+__device__ __forceinline__ void ffma2(float& c0, float& c1, float a, float b0, float b1) {
+  unsigned long long cc, aa, bb;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(cc) : "f"(c0), "f"(c1));
+  asm("mov.b64 %0, {%1, %2};" : "=l"(aa) : "f"(a), "f"(a));
+  asm("mov.b64 %0, {%1, %2};" : "=l"(bb) : "f"(b0), "f"(b1));
+  asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(cc) : "l"(aa), "l"(bb));
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(c0), "=f"(c1) : "l"(cc));
+}
+
 // Per-lane accumulator of V output elements.
 template <int DT, bool COMP, int V>
 struct SpmmAcc {
@@ -122,8 +133,13 @@ struct SpmmAcc {
       }
     } else {
       const R ar = to_real(a);
+      if constexpr (!COMP && std::is_same<R, float>::value && V % 2 == 0) {
 #pragma unroll
-      for (int j = 0; j < V; ++j) term(s[0][j], ar, to_real(b[j]));
+        for (int j = 0; j < V; j += 2) ffma2(s[0][j].hi, s[0][j + 1].hi, ar, to_real(b[j]), to_real(b[j + 1]));
+      } else {
+#pragma unroll
+        for (int j = 0; j < V; ++j) term(s[0][j], ar, to_real(b[j]));
+      }
     }
   }
 
