@@ -706,6 +706,7 @@ class BatchedMix:
 CASES = {
     "batched_f32": lambda d: BatchedMix(d),
     "bsr16_bf16_N128": lambda d: Bsr16(d, 128),
+    "bsr16_bf16_N64": lambda d: Bsr16(d, 64),
     "bsr_spmv_f32_bd16": lambda d: BsrSpmv(d),
     "spmv_f64": lambda d: SpmvZipf64(d),
     "spmm_f32_N64": lambda d: SpmmPowerLaw(d, "f32", 64),

@@ -23,6 +23,9 @@
 //    accumulator's "full" mbarrier;
 //  * warps 0-3 read their 32 TMEM lanes (= 32 dense columns) with tcgen05.ld,
 //    release the accumulator and store 16 output rows.
+// N may be any multiple of 64: in a last tile with only 64 columns left, the
+// upper half of each B slab is not loaded (its MMA rows compute unused values
+// from whatever that half of the slot holds, and are never stored).
 // Every mbarrier wait is bounded; on expiry a role records an error and stops,
 // the others run out their own bounded waits, and TMEM is freed on exit.
 #include <cstdint>
@@ -164,7 +167,7 @@ template <typename S>
 __global__ void __launch_bounds__(kBsrThreads, 4)
 k_bsr16_spmm(const __grid_constant__ CUtensorMap tmap_b, const S* __restrict__ packed, const int32_t* __restrict__ bcol,
              const int64_t* __restrict__ bptr, int64_t n_brows, int64_t rows_per_cta, S* __restrict__ C, int64_t ldc,
-             uint32_t idesc, int* __restrict__ err) {
+             int64_t n, uint32_t idesc, int* __restrict__ err) {
   extern __shared__ unsigned char smem_raw[];
   const uint32_t raw = smem_addr(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
@@ -180,7 +183,10 @@ k_bsr16_spmm(const __grid_constant__ CUtensorMap tmap_b, const S* __restrict__ p
   const int64_t col0 = int64_t(blockIdx.y) * kBsrTileM;
   const int64_t b0 = bptr[r0], total = bptr[r1] - b0;
 
-  if (warp < 4) {  // block rows without blocks get zero rows
+  // a tile's upper 64 columns may lie past N (N a multiple of 64): that half of
+  // the B slab is neither loaded nor stored
+  const bool upper = col0 + 64 < n;
+  if (warp < 4 && col0 + tid < n) {  // block rows without blocks get zero rows
     for (int64_t r = r0; r < r1; ++r) {
       if (bptr[r] == bptr[r + 1]) {
         S* c = C + r * 16 * ldc + col0 + tid;
@@ -226,9 +232,9 @@ k_bsr16_spmm(const __grid_constant__ CUtensorMap tmap_b, const S* __restrict__ p
         const int32_t krow = __ldg(bcol + blk) * 16;
         const uint32_t full = full0 + 8 * s;
         const uint32_t slab = base + kSmemSlabs + s * kSlabBytes;
-        mbar_arrive_expect_tx(full, kSlabBytes + kBlkBytes);
+        mbar_arrive_expect_tx(full, (upper ? kSlabBytes : kSlabBytes / 2) + kBlkBytes);
         tma_load_2d(slab, &tmap_b, static_cast<int32_t>(col0), krow, full);
-        tma_load_2d(slab + 2048, &tmap_b, static_cast<int32_t>(col0 + 64), krow, full);
+        if (upper) tma_load_2d(slab + 2048, &tmap_b, static_cast<int32_t>(col0 + 64), krow, full);
         bulk_load(base + kSmemBlocks + s * kBlkBytes, packed + blk * 256, kBlkBytes, full);
       }
     }
@@ -285,9 +291,11 @@ k_bsr16_spmm(const __grid_constant__ CUtensorMap tmap_b, const S* __restrict__ p
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(acce0 + 8 * buf);
-      S* c = C + r * 16 * ldc + col0 + warp * 32 + lane;
+      if (col0 + warp * 32 + lane < n) {
+        S* c = C + r * 16 * ldc + col0 + warp * 32 + lane;
 #pragma unroll
-      for (int n = 0; n < 16; ++n) store_out(c + n * ldc, __uint_as_float(v[n]));
+        for (int q = 0; q < 16; ++q) store_out(c + q * ldc, __uint_as_float(v[q]));
+      }
       ++rr;
     }
   }
@@ -340,14 +348,14 @@ int bsr_launch(CUtensorMapDataType tdt, uint32_t ab_format, const void* packed, 
              CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return FSB_ERR_UNSUPPORTED;
-  const int64_t tiles = n / kBsrTileM;
+  const int64_t tiles = ceil_div(n, kBsrTileM);
   const int64_t target = 148 * 4;  // resident CTAs: 4 per SM (registers)
   const int64_t rows_per_cta = ceil_div(n_brows, target);
   const int64_t grid_x = ceil_div(n_brows, rows_per_cta);
   dim3 grid((unsigned)grid_x, (unsigned)tiles);
   k_bsr16_spmm<S><<<grid, kBsrThreads, kSmemBytes, st>>>(map, static_cast<const S*>(packed), bcol, bptr, n_brows,
-                                                         rows_per_cta, static_cast<S*>(C), ldc, umma_idesc(ab_format),
-                                                         err);
+                                                         rows_per_cta, static_cast<S*>(C), ldc, n,
+                                                         umma_idesc(ab_format), err);
   FSB_LAUNCH_CHECK();
   return FSB_OK;
 }
@@ -379,11 +387,11 @@ int fsb_bsr16_spmm(int dtype, const void* packed, const int32_t* bcol, const int
   if (n_brows == 0 || n == 0) return FSB_OK;
   if (!bptr || !C || !d_error || (n_bcols > 0 && (!B || !packed || !bcol))) return FSB_ERR_INVALID_ARG;
   // TMA and bulk copies: B and the packed blocks 16-byte aligned, row stride a
-  // multiple of 16 bytes, whole 128-column tiles
-  if (n % kBsrTileM != 0 || ldb % 8 != 0 || reinterpret_cast<uintptr_t>(B) % 16 != 0 ||
+  // multiple of 16 bytes, whole 64-column TMA boxes
+  if (n % 64 != 0 || ldb % 8 != 0 || reinterpret_cast<uintptr_t>(B) % 16 != 0 ||
       reinterpret_cast<uintptr_t>(packed) % 16 != 0 || n_bcols * 16 > INT32_MAX || n > INT32_MAX)
     return FSB_ERR_UNSUPPORTED;
-  if (n / kBsrTileM > 65535) return FSB_ERR_UNSUPPORTED;
+  if (ceil_div(n, kBsrTileM) > 65535) return FSB_ERR_UNSUPPORTED;
   if (n_bcols == 0) {  // every block row is empty: C = 0 (no tensor map over an empty B)
     return cudaMemset2DAsync(C, size_t(ldc) * 2, 0, size_t(n) * 2, size_t(n_brows) * 16,
                              static_cast<cudaStream_t>(stream)) == cudaSuccess

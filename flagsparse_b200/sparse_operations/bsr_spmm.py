@@ -4,8 +4,8 @@ FlagSparse has no BSR SpMM (its BSR support is SpMV, ``spmv_bsr.py``); this
 operator serves matrices whose nonzeros come in dense 16 x 16 blocks, where a
 block times a 16-row slab of B is a real dense contraction.  Values and B are
 bfloat16 or float16; products accumulate in fp32 in tensor memory and C is
-written in the value type.  Dense widths are multiples of 128 (one tcgen05.mma
-covers 128 columns).
+written in the value type.  Dense widths are multiples of 64 (one tcgen05.mma
+covers a 128-column tile; a last tile of 64 columns loads and stores half).
 """
 
 import torch
@@ -95,8 +95,8 @@ def flagsparse_spmm_bsr16(blocks=None, indices=None, indptr=None, B=None, shape=
     if not B.is_cuda or B.device != prepared.blocks.device:
         raise ValueError("B must be a CUDA tensor on the same device as the sparse matrix")
     n = int(B.shape[1])
-    if n % 128:
-        raise ValueError("B.shape[1] must be a multiple of 128 for the tensor-core BSR path")
+    if n % 64:
+        raise ValueError("B.shape[1] must be a multiple of 64 for the tensor-core BSR path")
     B = B.contiguous()
     M = prepared.shape[0]
     if out is not None:

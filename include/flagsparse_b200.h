@@ -329,9 +329,10 @@ FSB_API int fsb_sddmm_csr(int dtype, const int32_t* row_ids, const int32_t* indi
  * bcol: int32 block columns; bptr: int64 block row pointers [n_brows + 1];
  * B: (16 n_bcols) x n row-major, row stride ldb, 16-byte aligned, read with
  * TMA; C: (16 n_brows) x n, row stride ldc, written in the value type (block
- * rows without blocks give zero rows).  n must be a multiple of 128 and ldb
- * of 8.  d_error (device int) is set to 1 if a bounded wait inside the
- * kernel expired.
+ * rows without blocks give zero rows).  n must be a multiple of 64 (a
+ * 128-column tile whose upper half lies past n loads and stores only its
+ * lower half) and ldb of 8.  d_error (device int) is set to 1 if a bounded
+ * wait inside the kernel expired.
  * No FlagSparse counterpart: its BSR support is SpMV (spmv_bsr.py).
  * ------------------------------------------------------------------------ */
 FSB_API int fsb_bsr16_pack(int dtype, const void* blocks, int64_t nnzb, void* packed, void* stream);

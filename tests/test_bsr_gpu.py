@@ -71,6 +71,8 @@ def _check(C, indptr, indices, blocks_r, B_r, dname, rows=None):
     (8, 8, 3, 128, ()),
     (64, 64, 8, 256, (3, 17)),
     (700, 900, 8, 384, (0, 699)),
+    (8, 8, 3, 64, (2,)),
+    (300, 200, 6, 192, (0, 299)),
 ])
 def test_bsr16_against_oracle(dt, n_brows, n_bcols, per_row, N, empty):
     indptr, indices, blocks = _case(n_brows, n_bcols, per_row, seed=n_brows + N, empty=empty)
@@ -138,8 +140,8 @@ def test_bsr16_validation_and_out():
     indptr, indices, blocks = _case(4, 4, 2, seed=1)
     args = (torch.from_numpy(blocks).bfloat16().cuda(), torch.from_numpy(indices).cuda(),
             torch.from_numpy(indptr).cuda())
-    with pytest.raises(ValueError, match="multiple of 128"):
-        fs.flagsparse_spmm_bsr16(*args, torch.randn(64, 64, device="cuda").bfloat16(), (64, 64))
+    with pytest.raises(ValueError, match="multiple of 64"):
+        fs.flagsparse_spmm_bsr16(*args, torch.randn(64, 96, device="cuda").bfloat16(), (64, 64))
     with pytest.raises(TypeError, match="bfloat16 or torch.float16"):
         fs.prepare_spmm_bsr16(args[0].float(), args[1], args[2], (64, 64))
     with pytest.raises(ValueError, match="multiples of 16"):
