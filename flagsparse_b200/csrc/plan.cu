@@ -378,9 +378,9 @@ int fsb_csr_inspect(const void* indices, int idx_is_64, const void* indptr, int 
                    : inspect_impl<int32_t, int32_t>(indices, indptr, n_rows, nnz, d_out, st);
 }
 
-// A row-block unit of a warp holds < 2*cap nonzeros: 16 per lane for the 2- and
-// 4-byte real types (cap 256), 8 per lane for the wider types (cap 128).
-int32_t fsb_spmv_default_cap(int dtype) { return (dtype == FSB_F16 || dtype == FSB_BF16 || dtype == FSB_F32) ? 256 : 128; }
+// A row-block unit of a warp holds < 2*cap nonzeros: 14 per lane for the 2- and
+// 4-byte real types (cap 224), 8 per lane for the wider types (cap 128).
+int32_t fsb_spmv_default_cap(int dtype) { return (dtype == FSB_F16 || dtype == FSB_BF16 || dtype == FSB_F32) ? 224 : 128; }
 
 // Long rows are cut into chunks of 256-nonzero batches per warp: four for the
 // 2- and 4-byte real types (fewer tickets on the gather-bound long rows), two

@@ -8,13 +8,14 @@
 //  * row-block units: a run of rows with < 2*cap nonzeros.  Persistent warps
 //    stride over the units, loading the next unit's descriptor and
 //    prefetching its values and columns into L2 while the current unit runs.
-//    Lanes load up to 16 nonzeros each with coalesced evict-first loads,
+//    Lanes load up to 14 nonzeros each with coalesced evict-first loads,
 //    gather x, park the products in the warp's shared-memory slice in
 //    compensated form, then a lane-level merge path sums the rows and a
 //    segmented shuffle scan joins rows that span lanes.
 //  * long-row chunks: `chunk_nnz` nonzeros of one row with > cap nonzeros, in
 //    256-nonzero batches whose column loads are issued one batch ahead; no
-//    shared memory.  A one-chunk row is written directly; otherwise the warp
+//    shared memory; launched as a programmatic dependent of the row-block
+//    launch so it overlaps that grid's tail.  A one-chunk row is written directly; otherwise the warp
 //    publishes a partial sum and the warp whose atomic ticket completes the
 //    row adds all partials in a fixed order and resets the ticket, so results
 //    are deterministic.
@@ -205,10 +206,13 @@ constexpr int kSpmvBatch = 32 * kSpmvItems;
 // Row-block units: nonzero slots per lane.  A unit holds < 2*cap nonzeros, so
 // the largest window is cap = 16 * slots.  Units carry a fixed cost (their
 // descriptor, row-pointer and first loads are dependent round trips), so the
-// 2- and 4-byte real types use 16 slots (cap 256); the wider types keep 8.
+// 2- and 4-byte real types use 14 slots (cap 224); the wider types keep 8.
+// 14 rather than 16: the smaller staging slice leaves more of each SM's L1 to
+// the long-row launch that overlaps this one's tail (199.7 against 210 us on
+// a 2 M-row Zipf matrix).
 template <int DT>
 struct SpmvRow {
-  static constexpr int kItems = (DT == FSB_F16 || DT == FSB_BF16 || DT == FSB_F32) ? 16 : 8;
+  static constexpr int kItems = (DT == FSB_F16 || DT == FSB_BF16 || DT == FSB_F32) ? 14 : 8;
   static constexpr int kBatch = 32 * kItems;
   static constexpr int kCap = kBatch / 2;
 };
@@ -250,6 +254,15 @@ struct SpmvLongMinBlocks {
   static constexpr int value =
       ((DT == FSB_F16 || DT == FSB_BF16 || DT == FSB_F32) && sizeof(IT) == 4) ? 5 : SpmvMinBlocks<DT>::value;
 };
+
+// The long-row launch may start while the row-block launch before it still
+// runs (programmatic dependent launch).  Its last block waits for that grid
+// before exiting, so the long-row grid completes only after both have: work
+// later in the stream sees every y row.  Waiting after its own work keeps
+// the overlap.
+__device__ __forceinline__ void spmv_long_join() {
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) asm volatile("griddepcontrol.wait;" ::: "memory");
+}
 
 // LONG = true: the long-row chunks units[unit0, unit1), no shared memory (the
 // gathers of long rows run faster with the L1 capacity that row-block staging
@@ -310,6 +323,7 @@ k_spmv_csr(const typename VT<DT>::Store* __restrict__ data, const IT* __restrict
     for (int m = 16; m > 0; m >>= 1) acc.shfl_combine(m);
     if (u.nch == 1) {
       if (lane == 0) y[u.row] = acc.result();
+      spmv_long_join();
       return;
     }
     const int64_t s0 = int64_t(u.slot) + (u.tag + 1);  // slot of this row's first chunk
@@ -321,7 +335,10 @@ k_spmv_csr(const typename VT<DT>::Store* __restrict__ data, const IT* __restrict
       ticket = atomicAdd(plan.counters + s0, 1);
     }
     ticket = __shfl_sync(0xffffffffu, ticket, 0);
-    if (ticket != u.nch - 1) return;
+    if (ticket != u.nch - 1) {
+      spmv_long_join();
+      return;
+    }
     __threadfence();
     Acc fin;
     fin.zero();
@@ -336,7 +353,11 @@ k_spmv_csr(const typename VT<DT>::Store* __restrict__ data, const IT* __restrict
       y[u.row] = fin.result();
       plan.counters[s0] = 0;  // ready for the next call
     }
+    spmv_long_join();
   } else {
+  // The long-row launch that follows is independent of this one (other rows,
+  // its own scratch): let it start on the SMs this grid leaves.
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   // -------------------------------------------------------------- row block
   // Persistent warps: units unit, unit + stride, ...; the next unit's
   // descriptor is loaded while the current one is processed, so only the
@@ -482,10 +503,24 @@ static int spmv_launch_mode(const void* data, const void* idx, const void* ptr, 
     FSB_LAUNCH_CHECK();
   }
   if (nu > nb) {  // long-row chunks: no shared memory
-    k_spmv_csr<DT, IT, PT, SHORT_COMP, true><<<(unsigned)ceil_div(nu - nb, kSpmvWarps), kSpmvWarps * 32, 0, st>>>(
-        static_cast<const S*>(data), static_cast<const IT*>(idx), static_cast<const PT*>(ptr),
-        static_cast<const S*>(x), static_cast<S*>(y), plan, nb, nu);
-    FSB_LAUNCH_CHECK();
+    // after a row-block launch: a programmatic dependent launch, so its blocks
+    // fill the SMs the row-block grid's tail leaves (see spmv_long_join)
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)ceil_div(nu - nb, kSpmvWarps));
+    cfg.blockDim = dim3(kSpmvWarps * 32);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = nb > 0 ? 1 : 0;
+    if (cudaLaunchKernelEx(&cfg, k_spmv_csr<DT, IT, PT, SHORT_COMP, true>, static_cast<const S*>(data),
+                           static_cast<const IT*>(idx), static_cast<const PT*>(ptr), static_cast<const S*>(x),
+                           static_cast<S*>(y), plan, nb, nu) != cudaSuccess) {
+      (void)cudaGetLastError();
+      return FSB_ERR_LAUNCH;
+    }
   }
   return FSB_OK;
 }

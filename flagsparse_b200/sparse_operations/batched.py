@@ -33,7 +33,7 @@ from .. import _native as nat
 from . import _csr
 
 # SpMV windows are given as fractions of the value type's largest window
-# (fsb_spmv_default_cap: 256 for 2- and 4-byte real types, 128 otherwise).
+# (fsb_spmv_default_cap: 224 for 2- and 4-byte real types, 128 otherwise).
 SPMV_CANDIDATES = ({"cap": 1, "chunk": 512}, {"cap": 2, "chunk": 512}, {"cap": 4, "chunk": 512},
                    {"cap": 1, "chunk": 1024})
 SPMM_CANDIDATES = ({"cap": 64, "chunk": 256}, {"cap": 32, "chunk": 256}, {"cap": 16, "chunk": 256},

@@ -198,7 +198,7 @@ typedef struct fsb_spmv_plan {
  * compensated.  Off by default. */
 #define FSB_SPMV_FAST_SHORT_ROWS 1
 
-/* Row-block window: 256 for f16 / bf16 / f32 (16 nonzeros per lane), 128 for
+/* Row-block window: 224 for f16 / bf16 / f32 (14 nonzeros per lane), 128 for
  * the wider types; any smaller window is accepted. */
 FSB_API int32_t fsb_spmv_default_cap(int dtype);
 /* Long-row chunk: 1024 nonzeros for f16 / bf16 / f32, 512 for the wider types;

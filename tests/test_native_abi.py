@@ -44,7 +44,7 @@ def test_size_queries_need_no_gpu():
     assert lib.fsb_spmv_partial_bytes(2) == 8
     assert lib.fsb_spmv_partial_bytes(5) == 32
     assert lib.fsb_spmv_partial_bytes(42) == -1
-    assert lib.fsb_spmv_default_cap(2) == 256 and lib.fsb_spmv_default_cap(3) == 128
+    assert lib.fsb_spmv_default_cap(2) == 224 and lib.fsb_spmv_default_cap(3) == 128
     assert lib.fsb_spmv_default_chunk(2) % 256 == 0
     assert lib.fsb_spmv_plan_workspace_bytes(10_000) > 0
     assert lib.fsb_csr_transpose_workspace_bytes(1 << 40, 10, 10) == -1
