@@ -15,7 +15,8 @@ import numpy as np
 import torch
 import torch.distributed as dist
 
-from .sparse_operations.spmm_csr import flagsparse_spmm_csr
+from .sparse_operations import _csr
+from .sparse_operations.spmm_csr import _prepare_spmm_csr_matrix
 from .sparse_operations.spmv_csr import flagsparse_spmv_csr, prepare_spmv_csr
 
 
@@ -80,6 +81,14 @@ class ShardedCsr:
         self.data = data[a:b].to(device)
         self.local_shape = (r1 - r0, self.shape[1])
         self.prepared = prepare_spmv_csr(self.data, self.indices, self.indptr, self.local_shape)
+        self._spmm = None  # (data, int32 indices, int64 indptr, SpmmPlan), built on the first spmm
+
+    def _spmm_operands(self):
+        if self._spmm is None:
+            data, ind, ptr, n_rows, n_cols, _rl, _mx = _prepare_spmm_csr_matrix(
+                self.data, self.indices, self.indptr, self.local_shape)
+            self._spmm = (data, ind, ptr, _csr.SpmmPlan(ptr, n_rows, data.dtype))
+        return self._spmm
 
     def spmv(self, x, gather=False, out=None):
         """y rows [row_begin, row_end) of A x (every row of A x with ``gather``)."""
@@ -87,6 +96,16 @@ class ShardedCsr:
         return gather_rows(y, self.shards, self.group) if gather else y
 
     def spmm(self, B, gather=False):
-        """C rows [row_begin, row_end) of A B (every row with ``gather``)."""
-        C = flagsparse_spmm_csr(self.data, self.indices, self.indptr, B, self.local_shape)
+        """C rows [row_begin, row_end) of A B (every row with ``gather``).
+
+        The shard is validated and its SpMM plan built once, on the first call.
+        """
+        data, ind, ptr, plan = self._spmm_operands()
+        if B.ndim != 2 or B.shape[0] != self.shape[1]:
+            raise ValueError(f"B must be 2D with B.shape[0] == n_cols={self.shape[1]}")
+        if B.dtype != data.dtype or B.device != data.device:
+            raise TypeError("B must match the matrix dtype and device")
+        B = B.contiguous()
+        C = torch.empty((self.local_shape[0], int(B.shape[1])), dtype=data.dtype, device=data.device)
+        _csr.spmm(data, ind, ptr, self.local_shape[0], self.shape[1], B, plan, C)
         return gather_rows(C, self.shards, self.group) if gather else C

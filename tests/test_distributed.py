@@ -91,7 +91,9 @@ def test_sharded_products_on_one_gpu(world):
     for rank in range(world):
         sh = fsd.ShardedCsr(data, indices, indptr, c["shape"], rank=rank, world_size=world)
         ys.append(sh.spmv(x))
-        Cs.append(sh.spmm(B))
+        first = sh.spmm(B)
+        Cs.append(sh.spmm(B))  # the second call reuses the shard's SpMM plan and scratch
+        assert torch.equal(first, Cs[-1])
     y = host(torch.cat(ys)).astype(np.float64)
     C = host(torch.cat(Cs)).astype(np.float64)
     d = c["data"].astype(np.float64)
