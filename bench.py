@@ -440,9 +440,11 @@ class AutogradChungLu:
     """Y = A X forward and dX = A^T dY, dvals = SDDMM(dY, X) backward on the 500,000-node
     Chung-Lu graph (mean degree 25, seed 3), 128 features.
 
-    Bytes per step, gather model: forward and backward SpMM each
-    nnz*(s_v+4) + (n+1)*8 + nnz*128*s + n*128*s, plus the SDDMM
-    2*nnz*128*s + nnz*(4+4) + nnz*s.
+    Bytes per step, gather model: the forward SpMM
+    nnz*(s_v+4) + (n+1)*8 + nnz*128*s + n*128*s, and the one-launch backward
+    nnz*(4+s_v+4) + (n+1)*8 + nnz*128*s + 2*n*128*s + nnz*s (permutation,
+    values through it, columns, row pointers, one dY gather per nonzero, X
+    and dX rows, dvals).  The SDDMM alone: 2*nnz*128*s + nnz*(4+4) + nnz*s.
     """
 
     def __init__(self, device, dname="bf16", part="fwd_bwd"):
@@ -483,7 +485,8 @@ class AutogradChungLu:
         s, n, z = self.s, self.n, self.nnz
         spmm = z * (s + 4) + (n + 1) * 8 + z * 128 * s + n * 128 * s
         sddmm = 2 * z * 128 * s + z * 8 + z * s
-        return sddmm if self.part == "sddmm" else 2 * spmm + sddmm
+        bwd = z * (4 + s + 4) + (n + 1) * 8 + z * 128 * s + 2 * n * 128 * s + z * s
+        return sddmm if self.part == "sddmm" else spmm + bwd
 
     def step(self):
         if self.part == "sddmm":
@@ -719,9 +722,9 @@ CASES = {
 }
 
 
-# native kernels per step: the SpMM layer's backward gathers A^T's values,
-# runs the transposed SpMM and the SDDMM after the forward SpMM.
-LAUNCHES_PER_STEP = {"autograd_f32": 4, "autograd_bf16": 4}
+# native kernels per step: the forward SpMM and the one-launch backward
+# (dX and dvals from fsb_spmm_csr_backward).
+LAUNCHES_PER_STEP = {"autograd_f32": 2, "autograd_bf16": 2}
 
 
 def measure_extras(torch, device, flush, peak):

@@ -123,7 +123,12 @@ _SIGNATURES = {
         [_c_int, _c_ptr, _c_ptr, _c_ptr, _c_i64, _c_i64, _c_ptr, _c_i64, _c_i64, _c_ptr, _c_i64, _c_ptr, _c_ptr,
          ctypes.POINTER(SpmvPlan), _c_ptr],
     ),
-    "fsb_csr_row_ids": (_c_int, [_c_ptr, _c_int, _c_i64, _c_i64, _c_ptr, _c_ptr]),
+    "fsb_spmm_csr_backward": (
+        _c_int,
+        [_c_int, _c_ptr, _c_ptr, _c_ptr, _c_ptr, _c_i64, _c_i64, _c_ptr, _c_i64, _c_ptr, _c_i64, _c_i64, _c_ptr,
+         _c_i64, _c_ptr, ctypes.POINTER(SpmvPlan), _c_ptr],
+    ),
+    "fsb_csr_row_ids":(_c_int, [_c_ptr, _c_int, _c_i64, _c_i64, _c_ptr, _c_ptr]),
     "fsb_sddmm_csr": (
         _c_int,
         [_c_int, _c_ptr, _c_ptr, _c_i64, _c_ptr, _c_i64, _c_ptr, _c_i64, _c_i64, _c_ptr,

@@ -301,6 +301,31 @@ def spmm_spmv(data, indices, indptr, n_rows, n_cols, B, plan, out, x, y, compens
     return True
 
 
+def _ld(t, n):
+    return int(t.stride(0)) if t.shape[0] > 1 else max(n, 1)
+
+
+def spmm_backward(vals, perm32, t_indices, t_indptr, n_rows, n_cols, dY, X, dX, dvals, t_plan):
+    """dX = A^T dY and, when ``dvals`` is given, dvals = <dY[row(p)], X[col(p)]> in one
+    launch through fsb_spmm_csr_backward.
+
+    ``vals`` are A's values (A order), ``perm32`` int32 with A's position of each
+    nonzero of A^T, ``t_plan`` A^T's SpmmPlan.  Returns False (nothing launched)
+    when the kernel does not apply (complex values, rows wider than 512 bytes,
+    unaligned rows); the caller then runs the separate kernels.
+    """
+    n = int(dY.shape[1])
+    rc = nat.lib().fsb_spmm_csr_backward(
+        nat.dtype_code(vals.dtype), nat.ptr(vals), nat.ptr(perm32), nat.ptr(t_indices), nat.ptr(t_indptr),
+        int(n_rows), int(n_cols), nat.ptr(dY), _ld(dY, n), nat.ptr(X), _ld(X, n) if X is not None else 0, n,
+        nat.ptr(dX), _ld(dX, n), nat.ptr(dvals), t_plan.struct_for(n), nat.stream_of(dX.device),
+    )
+    if rc == nat.FSB_ERR_UNSUPPORTED:
+        return False
+    nat.check(rc, "fsb_spmm_csr_backward")
+    return True
+
+
 def spmm(data, indices, indptr, n_rows, n_cols, B, plan, out, compensated=False):
     """out[:n_rows, :N] = A @ B through fsb_spmm_csr.
 

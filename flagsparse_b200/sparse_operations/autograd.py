@@ -3,12 +3,16 @@
 FlagSparse has no autograd for its CSR operators; this module provides the
 backward pass a training loop needs around ``flagsparse_spmm_csr``:
 
-  dX    = A^T dY   -- fsb_spmm_csr over the transposed pattern, built once
-                      (stable native transpose) and reused; the transposed
-                      values are regathered each backward, so A's values may
-                      change between steps
+  dX    = A^T dY   over the transposed pattern, built once (stable native
+                      transpose) and reused; A's values are read through the
+                      transpose permutation each backward, so they may change
+                      between steps
   dvals = SDDMM(dY, X) on A's pattern: dvals[p] = <dY[row(p)], X[col(p)]>
-                      -- fsb_sddmm_csr
+
+Both come from one launch of fsb_spmm_csr_backward, which gathers each dY row
+once for the two sums.  Where that kernel does not apply (rows wider than 512
+bytes, unaligned rows) the backward runs fsb_gather_values + fsb_spmm_csr for
+dX and fsb_sddmm_csr for dvals.
 
 Values and dense operands may be float16, bfloat16, float32 or float64; all
 products accumulate in fp32 (fp64 for float64).
@@ -27,7 +31,7 @@ class PreparedCsrSpmmAutograd:
     """A's pattern with everything forward and backward need, built once."""
 
     __slots__ = ("indices", "indptr", "shape", "n_rows", "n_cols", "nnz", "dtype", "row_ids", "t_indices",
-                 "t_indptr", "perm", "plan", "t_plan")
+                 "t_indptr", "perm", "perm32", "plan", "t_plan")
 
     def __init__(self, indices, indptr, shape, dtype):
         self.indices = indices
@@ -44,6 +48,8 @@ class PreparedCsrSpmmAutograd:
             self.t_indices = torch.empty(0, dtype=torch.int32, device=indices.device)
             self.t_indptr = torch.zeros(self.n_cols + 1, dtype=torch.int64, device=indices.device)
             self.perm = torch.empty(0, dtype=torch.int64, device=indices.device)
+        # the one-launch backward reads A's values through an int32 permutation
+        self.perm32 = self.perm.to(torch.int32) if 0 < self.nnz < 2**31 else None
         self.plan = _csr.SpmmPlan(indptr, self.n_rows, dtype)
         self.t_plan = _csr.SpmmPlan(self.t_indptr, self.n_cols, dtype)
 
@@ -84,6 +90,13 @@ class CsrSpmmFunction(torch.autograd.Function):
         p = ctx.prepared
         dY = dY.contiguous()
         d_vals = d_X = None
+        if ctx.needs_input_grad[1] and p.perm32 is not None:
+            d_X = torch.empty((p.n_cols, X.shape[1]), dtype=X.dtype, device=X.device)
+            d_vals = torch.empty_like(vals) if ctx.needs_input_grad[0] else None
+            if _csr.spmm_backward(vals, p.perm32, p.t_indices, p.t_indptr, p.n_rows, p.n_cols, dY,
+                                  X if d_vals is not None else None, d_X, d_vals, p.t_plan):
+                return d_vals, d_X, None
+            d_vals = d_X = None
         if ctx.needs_input_grad[1]:
             d_X = _spmm(p, vals, dY, transpose=True)
         if ctx.needs_input_grad[0]:

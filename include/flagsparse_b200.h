@@ -297,6 +297,27 @@ FSB_API int fsb_spmm_spmv_csr(int dtype, const void* data, const int32_t* indice
                       int64_t n_rows, int64_t n_cols, const void* B, int64_t ldb, int64_t n, void* C, int64_t ldc,
                       const void* x, void* y, const fsb_spmv_plan* plan, void* stream);
 
+/* Backward of Y = A X (A: n_rows x n_cols CSR with values vals[nnz]) in one
+ * launch over the transposed pattern (t_indices int32[nnz], t_indptr
+ * int64[n_cols + 1], and perm int32[nnz] with perm[q] = A's position of A^T's
+ * nonzero q, as fsb_csr_transpose gives them):
+ *   dX    = A^T dY                         (n_cols x n, row stride lddx)
+ *   dvals[p] = <dY[row(p)], X[col(p)]>     (when dvals is not NULL)
+ * dY is n_rows x n (stride lddy), X is n_cols x n (stride ldx).  Each dY row
+ * slice is gathered once for both sums, and A's values are read through perm
+ * (no transposed copy).  Real dtypes; needs 1 <= n, n * sizeof(value) <= 512,
+ * n a multiple of 16 / sizeof(value), 16-byte aligned dY, dX (and X) with such
+ * leading dimensions, and t_plan without FSB_SPMM_COMPENSATED.  Returns
+ * FSB_ERR_UNSUPPORTED otherwise, with nothing launched; the caller then runs
+ * fsb_gather_values + fsb_spmm_csr and fsb_sddmm_csr.  t_plan: A^T's SpMM plan
+ * with scratch for this n (as for fsb_spmm_csr).  dX sums in fp32 (fp64 for
+ * f64) in a fixed order; each dvals entry sums in fp32 (fp64) over a fixed
+ * tree.  No FlagSparse counterpart: it has no autograd for CSR SpMM. */
+FSB_API int fsb_spmm_csr_backward(int dtype, const void* vals, const int32_t* perm, const int32_t* t_indices,
+                          const int64_t* t_indptr, int64_t n_rows, int64_t n_cols, const void* dY, int64_t lddy,
+                          const void* X, int64_t ldx, int64_t n, void* dX, int64_t lddx, void* dvals,
+                          const fsb_spmv_plan* t_plan, void* stream);
+
 /* ------------------------------------------------------------------------
  * CSR SDDMM  out[p] = alpha * <x[row(p)], y[col(p)]> + beta * in[p].
  *
