@@ -30,7 +30,7 @@ SUPPORTED_AUTOGRAD_DTYPES = (torch.float16, torch.bfloat16, torch.float32, torch
 class PreparedCsrSpmmAutograd:
     """A's pattern with everything forward and backward need, built once."""
 
-    __slots__ = ("indices", "indptr", "shape", "n_rows", "n_cols", "nnz", "dtype", "row_ids", "t_indices",
+    __slots__ = ("indices", "indptr", "shape", "n_rows", "n_cols", "nnz", "dtype", "_row_ids", "t_indices",
                  "t_indptr", "perm", "perm32", "plan", "t_plan")
 
     def __init__(self, indices, indptr, shape, dtype):
@@ -40,7 +40,7 @@ class PreparedCsrSpmmAutograd:
         self.n_rows, self.n_cols = self.shape
         self.nnz = int(indices.numel())
         self.dtype = dtype
-        self.row_ids = _build_row_ids(indptr)
+        self._row_ids = None
         if self.nnz > 0:
             self.t_indices, self.t_indptr, self.perm = _csr.transpose_pattern(indices, indptr, self.shape,
                                                                               torch.int32, torch.int64)
@@ -52,6 +52,13 @@ class PreparedCsrSpmmAutograd:
         self.perm32 = self.perm.to(torch.int32) if 0 < self.nnz < 2**31 else None
         self.plan = _csr.SpmmPlan(indptr, self.n_rows, dtype)
         self.t_plan = _csr.SpmmPlan(self.t_indptr, self.n_cols, dtype)
+
+    @property
+    def row_ids(self):
+        """Row of every nonzero (int32), built on first use: only the separate SDDMM needs it."""
+        if self._row_ids is None:
+            self._row_ids = _build_row_ids(self.indptr)
+        return self._row_ids
 
 
 def prepare_spmm_csr_autograd(data, indices, indptr, shape):
