@@ -387,8 +387,11 @@ k_spmm_csr(const typename VT<DT>::Store* __restrict__ data, const int32_t* __res
 }
 
 // ---------------------------------------------------------------------------
-// Narrow dense rows (N * sizeof(value) <= 256 bytes): teams of T lanes own
-// 16-byte column slices and whole rows, G = 32 / T teams per warp.
+// Dense rows of at most 512 bytes (N * sizeof(value) <= 512, whole aligned
+// 16-byte slices): teams of T lanes (1 to 32) own 16-byte column slices and
+// whole rows, G = 32 / T teams per warp.  At 512 bytes (one team per warp) this
+// still beats k_spmm_csr by keeping 8 fp32 B slices of a row in flight
+// (fp32 N = 128 on a 1M-row power-law matrix: 2.13 ms against 2.26 ms).
 //  * row block: team g takes rows g, g+G, ... of the unit; the teams of a warp
 //    walk their rows together up to the longest of them (4 nonzeros ahead,
 //    inactive slots predicated off), so one load instruction moves G rows'
@@ -959,7 +962,7 @@ int spmm_dispatch(const void* data, const int32_t* idx, const int64_t* ptr, cons
   using S = typename VT<DT>::Store;
   constexpr int kVmax = 16 / int(sizeof(S));
   // narrow rows with whole, aligned 16-byte slices: teams of T lanes own rows
-  if (n * int64_t(sizeof(S)) <= 256 && n % kVmax == 0 && ldb % kVmax == 0 && ldc % kVmax == 0 &&
+  if (n * int64_t(sizeof(S)) <= 512 && n % kVmax == 0 && ldb % kVmax == 0 && ldc % kVmax == 0 &&
       reinterpret_cast<uintptr_t>(B) % 16 == 0 && reinterpret_cast<uintptr_t>(C) % 16 == 0) {
     int T = 1;
     while (int64_t(T) * kVmax < n) T *= 2;
