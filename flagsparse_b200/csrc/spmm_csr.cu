@@ -659,15 +659,34 @@ __device__ __forceinline__ void team_transpose_sum(R (&d)[M], int T, int tl, int
   writer = (tl & (2 * rest - 1)) == 0 || rest == 0;
 }
 
-// Per-lane partial dot products of the kA dY slices with this lane's X slice.
+// (c0, c1) += (a0 * b0, a1 * b1) in one packed fp32x2 FMA, each half rounded
+// as a scalar fma.rn.
+__device__ __forceinline__ void ffma2x(float& c0, float& c1, float a0, float a1, float b0, float b1) {
+  unsigned long long cc, aa, bb;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(cc) : "f"(c0), "f"(c1));
+  asm("mov.b64 %0, {%1, %2};" : "=l"(aa) : "f"(a0), "f"(a1));
+  asm("mov.b64 %0, {%1, %2};" : "=l"(bb) : "f"(b0), "f"(b1));
+  asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(cc) : "l"(aa), "l"(bb));
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(c0), "=f"(c1) : "l"(cc));
+}
+
+// Per-lane partial dot products of the kA dY slices with this lane's X slice
+// (already widened to R); fp32 sums run as two packed halves added at the end.
 template <typename S, typename R, int KA, int V>
-__device__ __forceinline__ void bwd_dots(const S (&bv)[KA][V], const S (&xs)[V], R (&d)[KA]) {
+__device__ __forceinline__ void bwd_dots(const S (&bv)[KA][V], const R (&xf)[V], R (&d)[KA]) {
 #pragma unroll
   for (int u = 0; u < KA; ++u) {
-    R s = R(0);
+    if constexpr (std::is_same<R, float>::value && V % 2 == 0) {
+      float s0 = 0.f, s1 = 0.f;
 #pragma unroll
-    for (int j = 0; j < V; ++j) s = fma(to_real(bv[u][j]), to_real(xs[j]), s);
-    d[u] = s;
+      for (int j = 0; j < V; j += 2) ffma2x(s0, s1, to_real(bv[u][j]), to_real(bv[u][j + 1]), xf[j], xf[j + 1]);
+      d[u] = s0 + s1;
+    } else {
+      R s = R(0);
+#pragma unroll
+      for (int j = 0; j < V; ++j) s = fma(to_real(bv[u][j]), xf[j], s);
+      d[u] = s;
+    }
   }
 }
 
@@ -742,8 +761,13 @@ k_spmm_bwd(const typename VT<DT>::Store* __restrict__ vals, const int32_t* __res
       const int len = has ? sh_off[i + 1] - b : 0;
       int maxlen = len;
       for (int m = T; m < 32; m <<= 1) maxlen = max(maxlen, __shfl_xor_sync(0xffffffffu, maxlen, m));
-      S xs[V];
-      if constexpr (DV) load_slice<S, V, true>(X + (int64_t(row) + (has ? i : 0)) * ldx + c0, len > 0 ? nv : 0, xs);
+      R xf[V];
+      if constexpr (DV) {
+        S xs[V];
+        load_slice<S, V, true>(X + (int64_t(row) + (has ? i : 0)) * ldx + c0, len > 0 ? nv : 0, xs);
+#pragma unroll
+        for (int j = 0; j < V; ++j) xf[j] = to_real(xs[j]);
+      }
       Acc acc;
       acc.zero();
       for (int k = 0; k < maxlen; k += kA) {
@@ -758,7 +782,7 @@ k_spmm_bwd(const typename VT<DT>::Store* __restrict__ vals, const int32_t* __res
           if (k + u < len) acc.add(sh_a[b + k + u], bv[u]);
         if constexpr (DV) {
           R d[kA];
-          bwd_dots<S, R, kA, V>(bv, xs, d);
+          bwd_dots<S, R, kA, V>(bv, xf, d);
           bwd_put_dots<S, R, kA>(d, b + k, 1, b + len, T, tl, sh_p, dvals);
         }
       }
@@ -773,8 +797,13 @@ k_spmm_bwd(const typename VT<DT>::Store* __restrict__ vals, const int32_t* __res
 
   // ------------------------------------------------------------ long-row chunk
   const int32_t nch = __ldg(&ud->n_chunks), slot = __ldg(&ud->slot);
-  S xs[V];
-  if constexpr (DV) load_slice<S, V, true>(X + int64_t(row) * ldx + c0, nv, xs);
+  R xf[V];
+  if constexpr (DV) {
+    S xs[V];
+    load_slice<S, V, true>(X + int64_t(row) * ldx + c0, nv, xs);
+#pragma unroll
+    for (int j = 0; j < V; ++j) xf[j] = to_real(xs[j]);
+  }
   Acc acc;
   acc.zero();
   for (int64_t b0 = s0; b0 < s1; b0 += kSpmmBatch) {
@@ -796,7 +825,7 @@ k_spmm_bwd(const typename VT<DT>::Store* __restrict__ vals, const int32_t* __res
       }
       if constexpr (DV) {
         R d[kA];
-        bwd_dots<S, R, kA, V>(bv, xs, d);
+        bwd_dots<S, R, kA, V>(bv, xf, d);
         bwd_put_dots<S, R, kA>(d, k + team, G, cnt, T, tl, sh_p, dvals);
       }
     }
