@@ -57,3 +57,37 @@ def test_invalid_arguments_are_rejected_without_touching_the_device():
     assert lib.fsb_spmv_plan_analyze(None, 0, -1, 1024, 4096, None, 0, None, None) == _native.FSB_ERR_INVALID_ARG
     assert lib.fsb_gather_values(2, None, None, 3, 0, None, None) == _native.FSB_ERR_INVALID_ARG
     assert lib.fsb_spmv_csr(2, None, None, 0, None, 0, 4, 4, None, None, None, None) == _native.FSB_ERR_INVALID_ARG
+
+
+def _declared_param_counts():
+    counts = {}
+    include = os.path.join(REPO, "include")
+    for fname in os.listdir(include):
+        if not fname.endswith(".h"):
+            continue
+        text = open(os.path.join(include, fname)).read()
+        for m in re.finditer(r"FSB_API\s+[A-Za-z_][A-Za-z0-9_ \*]*?\b(fsb_[a-z0-9_]+)\s*\(([^)]*)\)\s*;", text):
+            params = " ".join(m.group(2).split())
+            counts[m.group(1)] = 0 if params in ("", "void") else params.count(",") + 1
+    return counts
+
+
+def test_binding_argument_counts_match_the_header():
+    """Every ctypes signature has as many arguments as its C declaration."""
+    counts = _declared_param_counts()
+    assert set(counts) == set(_native.exported_symbols())
+    wrong = {n: (c, len(_native._SIGNATURES[n][1])) for n, c in counts.items() if c != len(_native._SIGNATURES[n][1])}
+    assert not wrong, wrong
+
+
+def test_backward_entry_rejects_bad_arguments_without_a_launch():
+    lib = _native.lib()
+    # no plan, negative width, missing dX: rejected on the host
+    assert lib.fsb_spmm_csr_backward(2, None, None, None, None, 4, 4, None, 8, None, 8, 8, None, 8, None, None,
+                                     None) == _native.FSB_ERR_INVALID_ARG
+    plan = _native.SpmvPlan()
+    assert lib.fsb_spmm_csr_backward(2, None, None, None, None, 4, 4, None, 8, None, 8, -1, None, 8, None,
+                                     ctypes.byref(plan), None) == _native.FSB_ERR_INVALID_ARG
+    # n == 0 is left to the separate kernels
+    assert lib.fsb_spmm_csr_backward(2, None, None, None, None, 4, 4, None, 8, None, 8, 0, ctypes.c_void_p(16), 8,
+                                     None, ctypes.byref(plan), None) == _native.FSB_ERR_UNSUPPORTED
