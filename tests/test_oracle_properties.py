@@ -9,7 +9,6 @@ limits.
 """
 
 import numpy as np
-import pytest
 from hypothesis import given, settings, strategies as st
 
 from oracle import oracle
