@@ -387,11 +387,12 @@ k_spmm_csr(const typename VT<DT>::Store* __restrict__ data, const int32_t* __res
 }
 
 // ---------------------------------------------------------------------------
-// Dense rows of at most 512 bytes (N * sizeof(value) <= 512, whole aligned
-// 16-byte slices): teams of T lanes (1 to 32) own 16-byte column slices and
-// whole rows, G = 32 / T teams per warp.  At 512 bytes (one team per warp) this
-// still beats k_spmm_csr by keeping 8 fp32 B slices of a row in flight
-// (fp32 N = 128 on a 1M-row power-law matrix: 2.13 ms against 2.26 ms).
+// Dense rows made of whole aligned 16-byte slices: teams of T lanes (1 to 32)
+// own 16-byte column slices and whole rows, G = 32 / T teams per warp; rows
+// wider than 512 bytes run 32-lane teams over 512-byte column tiles
+// (grid.y).  One team per warp still beats k_spmm_csr by keeping a row's B
+// slices in flight (1M-row power-law matrix: fp32 N = 128 2.11 ms against
+// 2.24 ms, fp32 N = 256 4.22 against 4.48, fp64 N = 128 4.54 against 10.85).
 //  * row block: team g takes rows g, g+G, ... of the unit; the teams of a warp
 //    walk their rows together up to the longest of them (4 nonzeros ahead,
 //    inactive slots predicated off), so one load instruction moves G rows'
@@ -437,7 +438,7 @@ k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __re
   const int64_t unit = int64_t(blockIdx.x) * kSpmmWarps + warp;
   if (unit >= plan.n_units) return;  // whole warp leaves together
   const int G = 32 / T, team = lane / T, tl = lane % T;
-  const int64_t c0 = int64_t(tl) * V;
+  const int64_t c0 = int64_t(blockIdx.y) * (T * V) + int64_t(tl) * V;  // rows wider than 32 lanes: 512-byte tiles
   const int nv = c0 + V <= n ? V : 0;  // n is a multiple of V
 
   unsigned char* wbase = smem_raw + warp * spmm_warp_smem_bytes<S>();
@@ -581,7 +582,7 @@ k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __re
   __threadfence();
   __syncwarp();
   int ticket = 0;
-  if (lane == 0) ticket = atomicAdd(plan.counters + first * cps, 1);
+  if (lane == 0) ticket = atomicAdd(plan.counters + first * cps + blockIdx.y, 1);
   ticket = __shfl_sync(0xffffffffu, ticket, 0);
   if (ticket != nch - 1) return;
   __threadfence();
@@ -603,7 +604,7 @@ k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __re
       put_y(y[row], fy.value());
     }
   }
-  if (lane == 0) plan.counters[first * cps] = 0;  // ready for the next call
+  if (lane == 0) plan.counters[first * cps + blockIdx.y] = 0;  // ready for the next call
 }
 
 // ---------------------------------------------------------------------------
@@ -915,11 +916,11 @@ int spmm_pick_v(const void* B, int64_t ldb, const void* C, int64_t ldc, int64_t 
 template <int DT, bool COMP, bool FUSED = false>
 int spmm_launch_team(const void* data, const int32_t* idx, const int64_t* ptr, const void* B, int64_t ldb, int64_t n,
                      void* C, int64_t ldc, const fsb_spmv_plan& plan, int T, cudaStream_t st,
-                     const void* x = nullptr, void* y = nullptr) {
+                     const void* x = nullptr, void* y = nullptr, int64_t tiles = 1) {
   using S = typename VT<DT>::Store;
   const int64_t blocks = ceil_div(plan.n_units, kSpmmWarps);
   const size_t smem = size_t(spmm_warp_smem_bytes<S>()) * kSpmmWarps;
-  k_spmm_team<DT, COMP, FUSED><<<(unsigned)blocks, kSpmmWarps * 32, smem, st>>>(
+  k_spmm_team<DT, COMP, FUSED><<<dim3((unsigned)blocks, (unsigned)tiles), kSpmmWarps * 32, smem, st>>>(
       static_cast<const S*>(data), idx, ptr, static_cast<const S*>(B), ldb, n, static_cast<S*>(C), ldc, plan, T,
       spmm_pstride(n), spmm_cps(n), static_cast<const S*>(x), static_cast<S*>(y));
   FSB_LAUNCH_CHECK();
@@ -997,6 +998,11 @@ int spmm_dispatch(const void* data, const int32_t* idx, const int64_t* ptr, cons
     while (int64_t(T) * kVmax < n) T *= 2;
     return spmm_launch_team<DT, COMP>(data, idx, ptr, B, ldb, n, C, ldc, plan, T, st);
   }
+  // wider rows of whole aligned slices: 32-lane teams over 512-byte column tiles
+  if (n % kVmax == 0 && ldb % kVmax == 0 && ldc % kVmax == 0 && reinterpret_cast<uintptr_t>(B) % 16 == 0 &&
+      reinterpret_cast<uintptr_t>(C) % 16 == 0 && ceil_div(n, int64_t(32) * kVmax) <= 65535)
+    return spmm_launch_team<DT, COMP>(data, idx, ptr, B, ldb, n, C, ldc, plan, 32, st, nullptr, nullptr,
+                                      ceil_div(n, int64_t(32) * kVmax));
   const int v = spmm_pick_v<DT>(B, ldb, C, ldc, n);
   if constexpr (kVmax >= 8)
     if (v == 8) return spmm_launch_v<DT, 8, COMP>(data, idx, ptr, B, ldb, n, C, ldc, plan, st);

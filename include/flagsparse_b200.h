@@ -261,11 +261,11 @@ FSB_API int fsb_spmv_csr_static_scratch(int dtype, const void* data, const void*
  *
  * Uses an fsb_spmv_plan built by fsb_spmv_plan_analyze / _build with
  * cap = fsb_spmm_default_cap (<= 64) and chunk_nnz = fsb_spmm_default_chunk
- * (a multiple of 128).  Rows of at most 512 bytes made of whole 16-byte
- * slices (16-byte aligned B and C, n, ldb and ldc multiples of the slice) run
- * on teams of lanes that own whole rows; otherwise one warp handles one (unit,
- * column tile) and its lanes own consecutive column groups, with 16-byte loads
- * where B, C, ldb and ldc are aligned for them.  Rows of several chunks reduce
+ * (a multiple of 128).  Rows made of whole 16-byte slices (16-byte aligned B
+ * and C, n, ldb and ldc multiples of the slice) run on teams of lanes that own
+ * whole rows (512-byte column tiles beyond 512 bytes); otherwise one warp
+ * handles one (unit, column tile) and its lanes own consecutive column groups,
+ * with loads as wide as B, C, ldb and ldc allow.  Rows of several chunks reduce
  * through the plan's
  * scratch, sized per slot by fsb_spmm_scratch_layout for this n:
  * partials = n_slots * partial_bytes_per_slot bytes, counters = n_slots *
