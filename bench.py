@@ -14,10 +14,13 @@ SpMV over the whole matrix.
   roofline  algorithmic bytes per launch / mean launch time vs measured HBM peak
   cpu_baseline  the CPU oracle on the host cores, bounded sample
 
-``--impl reference`` times the CPU restatement of the reference's SpMV
-semantics (fp32 values, fp64 row sums) with all host threads.
-Multi-GPU (torchrun): each rank runs an independent replica (weak scaling);
-there is no data-path collective.
+``--impl reference`` times the reference's CPU path for this operator:
+torch.sparse.mm on a CPU sparse_csr_tensor, fp32 values summed in fp64 as the
+reference's own fp32 tests compute their reference, with all host threads.
+The C restatement of the same semantics (oracle/) is reported beside it.
+Multi-GPU (torchrun): the headline SpMV splits the matrix by rows across the
+ranks (ShardedCsr, strong scaling, no data-path collective); the other
+``--case`` workloads run one independent replica per rank (weak scaling).
 """
 
 import argparse
@@ -144,6 +147,50 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(sel), "window": window, "source": self.source}
 
 
+# ---------------------------------------------------------------- the reference's CPU path
+
+class TorchCpuSpmv:
+    """y = A x on the host cores through torch.sparse.mm on a CPU sparse_csr_tensor: the
+    reference's CPU path.  fp32 values and x are summed in fp64 and y is rounded back to
+    fp32, as the reference's fp32 tests form their reference (tests/pytest/
+    test_spmm_csr_accuracy.py:108-117, test_spmv_csr_accuracy.py:52-59).  The fp64 copy
+    of A is made once (the reference caches its fp64 copy of the values too,
+    sparse_operations/spmv_csr.py:138-144); x is widened every step."""
+
+    def __init__(self, c, nthreads=None):
+        import torch
+
+        self.torch = torch
+        self.nthreads = int(nthreads or os.cpu_count() or 1)
+        torch.set_num_threads(self.nthreads)
+        self.A64 = torch.sparse_csr_tensor(torch.from_numpy(c["indptr"]), torch.from_numpy(c["indices"]),
+                                           torch.from_numpy(c["data"].astype(np.float64)), size=c["shape"])
+        self.x = torch.from_numpy(c["x"])
+
+    def step(self):
+        torch = self.torch
+        return torch.sparse.mm(self.A64, self.x.double()[:, None])[:, 0].float()
+
+
+def _wall_per_step(fn, budget_s, max_reps=400):
+    """Repeat fn() until ~budget_s seconds have passed; return (seconds per step, reps)."""
+    fn()
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        fn()
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or reps >= max_reps:
+            return el / reps, reps
+
+
+def spmv_zipf_config(M, K, nnz):
+    return {"workload": "spmv_csr_zipf2_2Mx2M_f32", "rows": M, "cols": K, "nnz": nnz,
+            "row_length": "min(50000, ceil(2.887*Z)), Z~Zipf(2) truncated at 50000",
+            "index_dtype": "int32", "indptr_dtype": "int64", "seed": 1,
+            "l2": "flushed between timed steps (256 MiB write, then a 50 us device spin that covers the host call)"}
+
+
 # ---------------------------------------------------------------- workloads
 
 class SpmvZipf:
@@ -181,10 +228,7 @@ class SpmvZipf:
         self.s_out = torch.cuda.Stream(device=device)
 
     def config(self):
-        return {"workload": self.name, "rows": self.M, "cols": self.K, "nnz": self.nnz,
-                "row_length": "min(50000, ceil(2.887*Z)), Z~Zipf(2) truncated at 50000",
-                "index_dtype": "int32", "indptr_dtype": "int64", "seed": 1,
-                "l2": "flushed between timed steps (256 MiB write, then a 50 us device spin that covers the host call)"}
+        return dict(spmv_zipf_config(self.M, self.K, self.nnz), workload=self.name)
 
     def alg_bytes(self):
         # values + column indices + row pointers + x once + y once
@@ -246,6 +290,61 @@ class SpmvZipf:
 
         c = self.host
         return oracle.spmv_f32_acc64(c["indptr"], c["indices"], c["data"], c["x"], nthreads=nthreads)
+
+
+class SpmvZipfSharded(SpmvZipf):
+    """The headline SpMV split across ranks by rows (flagsparse_b200.distributed.ShardedCsr):
+    each rank multiplies its block of rows (about nnz / world nonzeros) by the whole x and
+    keeps its rows of y.  The total work is fixed (strong scaling); value = the whole
+    matrix's bytes / the slowest rank's time."""
+
+    pipelined = False  # end-to-end steps run serially (upload, SpMV, download)
+
+    def __init__(self, device, rank, world, seed=1):
+        import torch
+
+        import flagsparse_b200 as fs
+        from flagsparse_b200 import distributed as fsd
+        from flagsparse_b200 import workloads
+
+        self.torch, self.fs = torch, fs
+        c = workloads.zipf_csr(n=2_000_000, seed=seed, dtype=np.float32)
+        self.host = c
+        self.M, self.K = c["shape"]
+        self.nnz = int(c["indices"].size)
+        self.device = device
+        self.sh = fsd.ShardedCsr(torch.from_numpy(c["data"]), torch.from_numpy(c["indices"]),
+                                 torch.from_numpy(c["indptr"]), c["shape"], rank=rank, world_size=world,
+                                 device=device)
+        self.prepared = self.sh.prepared
+        self.rows = self.sh.row_end - self.sh.row_begin
+        self.local_nnz = int(self.sh.indices.numel())
+        self.x = torch.from_numpy(c["x"]).to(device)
+        self.y = torch.empty(self.rows, dtype=torch.float32, device=device)
+        self.x_host = torch.from_numpy(c["x"]).pin_memory()
+        self.x_dev2 = torch.empty_like(self.x)
+        self.y_host = torch.empty(self.rows, dtype=torch.float32).pin_memory()
+
+    def config(self):
+        return dict(super().config(), split="rows balanced by nonzeros, x replicated, y row-sharded")
+
+    def alg_bytes(self):
+        # this rank's share: its values, columns, row pointers, the whole x and its rows of y
+        return self.local_nnz * 8 + (self.rows + 1) * 8 + self.K * 4 + self.rows * 4
+
+    def total_bytes(self):
+        return self.nnz * (4 + 4) + (self.M + 1) * 8 + self.K * 4 + self.M * 4
+
+    def step(self):
+        self.sh.spmv(self.x, out=self.y)
+
+    def e2e_step(self):
+        self.x_dev2.copy_(self.x_host, non_blocking=True)
+        self.sh.spmv(self.x_dev2, out=self.y)
+        self.y_host.copy_(self.y, non_blocking=True)
+
+    def e2e_bytes(self):
+        return self.K * 4, self.rows * 4
 
 
 class SpmvZipf64(SpmvZipf):
@@ -846,6 +945,8 @@ def main():
 
     if args.mtx:
         wl = SpmvMtx(device, args.mtx)
+    elif args.case == "spmv" and world > 1:
+        wl = SpmvZipfSharded(device, rank, world)
     else:
         wl = SpmvZipf(device) if args.case == "spmv" else CASES[args.case](device)
     headline = args.case == "spmv" and not args.mtx
@@ -879,7 +980,7 @@ def main():
     t_ms = sum(step_ms)
 
     # end-to-end through the public API with host buffers
-    pipelined = hasattr(wl, "e2e_run")
+    pipelined = hasattr(wl, "e2e_run") and getattr(wl, "pipelined", True)
     if pipelined:
         wl.e2e_run(2)
     else:
@@ -909,8 +1010,11 @@ def main():
         t_ms, e2e_ms = tt.tolist()
 
     alg = wl.alg_bytes()
-    value = world * alg * args.steps / (t_ms * 1e-3) / 1e9
-    e2e_val = world * alg * args.steps / (e2e_ms * 1e-3) / 1e9
+    # a sharded workload splits one fixed job (strong scaling); replicas repeat it per rank (weak)
+    job = wl.total_bytes() if hasattr(wl, "total_bytes") else world * alg
+    scaling = "strong" if hasattr(wl, "total_bytes") else "weak"
+    value = job * args.steps / (t_ms * 1e-3) / 1e9
+    e2e_val = job * args.steps / (e2e_ms * 1e-3) / 1e9
     peak, peak_src = _measured_peaks()
     mean_launch_ms = statistics.mean(step_ms)
     achieved = alg / (mean_launch_ms * 1e-3) / 1e9
@@ -921,15 +1025,21 @@ def main():
     if world == 1 and headline and not args.no_extras:
         extras = measure_extras(torch, device, flush, peak)
 
-    cpu = None
+    cpu = cpu_port = None
     if rank == 0 and world == 1 and headline and not args.no_cpu:
+        ref = TorchCpuSpmv(wl.host)
+        s_per, reps = _wall_per_step(ref.step, args.cpu_budget)
+        cpu = {"value": round(alg / s_per / 1e9, 3), "unit": "GB/s", "cores": ref.nthreads, "kind": "reference",
+               "sample": f"{reps} full SpMVs of the same matrix through torch.sparse.mm on a CPU sparse_csr_tensor "
+                         f"(the reference's CPU path; fp32 values summed in fp64), {s_per * 1e3:.1f} ms each"}
+        del ref
         from oracle import oracle
 
         nthreads = oracle.max_threads()
         s_per, reps = _cpu_measure(wl.cpu_run, args.cpu_budget, nthreads)
-        cpu = {"value": round(alg / s_per / 1e9, 3), "unit": "GB/s", "cores": nthreads, "kind": "port",
-               "sample": f"{reps} full SpMVs of the same matrix (fp32 values, fp64 row sums), "
-                         f"{s_per * 1e3:.1f} ms each, OpenMP over rows"}
+        cpu_port = {"value": round(alg / s_per / 1e9, 3), "unit": "GB/s", "cores": nthreads, "kind": "port",
+                    "sample": f"{reps} full SpMVs of the same matrix (fp32 values, fp64 row sums), "
+                              f"{s_per * 1e3:.1f} ms each, the C restatement, OpenMP over rows"}
 
     if rank == 0:
         line = {
@@ -941,13 +1051,14 @@ def main():
             "warmup": args.warmup,
             "ms_per_step": round(t_ms / args.steps, 5),
             "higher_is_better": True,
-            "scaling": "weak",
+            "scaling": scaling,
             "vs_baseline": None,
             "dtype": wl.dtype,
             "data": ("synthetic (seeded Zipf(2) power-law CSR, values/x U[-1,1])" if headline
                      else f"MatrixMarket file {os.path.basename(args.mtx)}, x U[-1,1]" if args.mtx
                      else "synthetic (seeded generators; see config.workload)"),
-            "config": dict(wl.config(), parallelism=f"replicas{world}" if world > 1 else "single"),
+            "config": dict(wl.config(), parallelism=(f"rows{world}" if scaling == "strong" else f"replicas{world}")
+                           if world > 1 else "single"),
             "e2e": {"value": round(e2e_val, 2), "unit": "GB/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
                     "schedule": ("pipelined: x upload of step i+1 and y download of step i-1 overlap "
@@ -958,6 +1069,7 @@ def main():
                          "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs, copy burst)",
                          "alg_bytes_per_launch": alg},
             "cpu_baseline": cpu,
+            "cpu_baseline_port": cpu_port,
             "gpu_launches": args.steps * (wl.launches_per_step() if hasattr(wl, "launches_per_step")
                                           else LAUNCHES_PER_STEP.get(args.case, 1)),
             "clocks": clocks,
@@ -970,7 +1082,9 @@ def main():
 
 
 def run_reference(args, rank, world):
-    """CPU restatement of the reference's SpMV semantics, all host threads, rank 0 only."""
+    """The reference's CPU path (torch.sparse.mm on a CPU sparse_csr_tensor, fp32 values summed
+    in fp64) on the headline matrix with all host threads, rank 0 only; the C restatement of
+    the same semantics is timed beside it."""
     if rank != 0:
         return
     from flagsparse_b200 import workloads
@@ -980,27 +1094,32 @@ def run_reference(args, rank, world):
     nnz = int(c["indices"].size)
     M, K = c["shape"]
     alg = nnz * 8 + (M + 1) * 8 + K * 4 + M * 4
-    nthreads = oracle.max_threads()
+    ref = TorchCpuSpmv(c)
     for _ in range(args.warmup):
-        oracle.spmv_f32_acc64(c["indptr"], c["indices"], c["data"], c["x"], nthreads=nthreads)
-    # each step is one full SpMV; cap the number of steps so the run stays short
+        ref.step()
     steps = args.steps
     t0 = time.perf_counter()
     for _ in range(steps):
-        oracle.spmv_f32_acc64(c["indptr"], c["indices"], c["data"], c["x"], nthreads=nthreads)
+        ref.step()
     el = time.perf_counter() - t0
     value = alg * steps / el / 1e9
+    nthreads = oracle.max_threads()
+    port_s, port_reps = _cpu_measure(
+        lambda nt: oracle.spmv_f32_acc64(c["indptr"], c["indices"], c["data"], c["x"], nthreads=nt),
+        min(args.cpu_budget, 5.0), nthreads)
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": steps,
         "warmup": args.warmup, "ms_per_step": round(el / steps * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded Zipf(2) power-law CSR, values/x U[-1,1])",
-        "config": {"workload": SpmvZipf.name, "rows": M, "cols": K, "nnz": nnz, "index_dtype": "int32",
-                   "parallelism": "host cores"},
+        "config": dict(spmv_zipf_config(M, K, nnz), parallelism=f"rows{world}" if world > 1 else "single"),
         "impl": "reference",
-        "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": nthreads, "kind": "port",
-                         "sample": f"{steps} full SpMVs, fp32 values with fp64 row sums (FlagSparse's fp32 "
-                                   "semantics), OpenMP over rows"},
+        "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": ref.nthreads, "kind": "reference",
+                         "sample": f"{steps} full SpMVs through torch.sparse.mm on a CPU sparse_csr_tensor "
+                                   "(the reference's CPU path), fp32 values summed in fp64"},
+        "cpu_baseline_port": {"value": round(alg / port_s / 1e9, 3), "unit": "GB/s", "cores": nthreads,
+                              "kind": "port", "sample": f"{port_reps} full SpMVs, the C restatement (fp32 values, "
+                                                        "fp64 row sums), OpenMP over rows"},
         "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))

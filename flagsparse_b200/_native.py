@@ -55,7 +55,7 @@ class SpmvPlan(ctypes.Structure):
         ("partials", _c_ptr),
         ("counters", _c_ptr),
         ("flags", _c_i32),
-        ("reserved", _c_i32),
+        ("tile_bytes", _c_i32),
     ]
 
 

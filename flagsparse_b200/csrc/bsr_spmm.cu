@@ -26,8 +26,11 @@
 // N may be any multiple of 64: in a last tile with only 64 columns left, the
 // upper half of each B slab is not loaded (its MMA rows compute unused values
 // from whatever that half of the slot holds, and are never stored).
-// Every mbarrier wait is bounded; on expiry a role records an error and stops,
-// the others run out their own bounded waits, and TMEM is freed on exit.
+// Every mbarrier wait is bounded.  On expiry a role records the error (in the
+// caller's error word and in a shared abort flag that every other wait polls)
+// and stops; before TMEM is freed the producer waits (bounded) for the copies
+// it issued to land and the MMA thread commits a drain barrier and waits
+// (bounded) for its issued MMAs, so no copy or MMA is left in flight.
 #include <cstdint>
 #include <mutex>
 
@@ -88,8 +91,9 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
 }
 
-// Returns false if the phase with the given parity did not complete within the poll limit.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// Returns false if the phase with the given parity did not complete within the
+// poll limit, or (when abort is given) once another role has set *abort.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const volatile int* abort = nullptr) {
   for (uint32_t i = 0; i < kWaitLimit; ++i) {
     uint32_t done;
     asm volatile(
@@ -98,6 +102,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
         : "r"(bar), "r"(parity)
         : "memory");
     if (done) return true;
+    if (abort && (i & 255u) == 255u && *abort) return false;
   }
   return false;
 }
@@ -158,13 +163,22 @@ __device__ __forceinline__ void store_out(__nv_bfloat16* p, float v) { *p = __fl
 __device__ __forceinline__ void store_out(__half* p, float v) { *p = __float2half_rn(v); }
 
 // Shared-memory map (from a 1024-byte aligned base): slabs [S][4096] | blocks
-// [S][512] | mbarriers full[S], empty[S], acc_full[2], acc_empty[2] | TMEM address.
+// [S][512] | mbarriers full[S], empty[S], acc_full[2], acc_empty[2], drain |
+// TMEM address | abort flag.
 constexpr int kSmemSlabs = 0;
 constexpr int kSmemBlocks = kBsrStages * kSlabBytes;
 constexpr int kSmemBars = kSmemBlocks + kBsrStages * kBlkBytes;
-constexpr int kNumBars = 2 * kBsrStages + 4;
+constexpr int kNumBars = 2 * kBsrStages + 5;
 constexpr int kSmemTmemSlot = kSmemBars + kNumBars * 8;
+constexpr int kSmemAbort = kSmemTmemSlot + 4;
 constexpr int kSmemBytes = 1024 + kSmemTmemSlot + 16;  // 1024: alignment slack for the base
+
+// A bounded wait expired: record it for the host (err may be device memory or
+// mapped pinned host memory, so a plain store) and tell the other roles.
+__device__ __forceinline__ void bsr_fail(int* err, volatile int* abort) {
+  *reinterpret_cast<volatile int*>(err) = 1;
+  *abort = 1;
+}
 
 // grid: x = CTAs over contiguous block-row ranges, y = 128-column tiles of C.
 template <typename S>
@@ -177,8 +191,9 @@ k_bsr16_spmm(const __grid_constant__ CUtensorMap tmap_b, const S* __restrict__ p
   const uint32_t base = (raw + 1023u) & ~1023u;
   unsigned char* smem = smem_raw + (base - raw);
   const uint32_t full0 = base + kSmemBars, empty0 = full0 + 8 * kBsrStages;
-  const uint32_t accf0 = empty0 + 8 * kBsrStages, acce0 = accf0 + 16;
+  const uint32_t accf0 = empty0 + 8 * kBsrStages, acce0 = accf0 + 16, drain = acce0 + 16;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(smem + kSmemTmemSlot);
+  volatile int* abort = reinterpret_cast<volatile int*>(smem + kSmemAbort);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int64_t r0 = int64_t(blockIdx.x) * rows_per_cta;
@@ -215,6 +230,8 @@ k_bsr16_spmm(const __grid_constant__ CUtensorMap tmap_b, const S* __restrict__ p
       mbar_init(accf0 + 8 * i, 1);
       mbar_init(acce0 + 8 * i, 4);  // one arrival per epilogue warp
     }
+    mbar_init(drain, 1);
+    *abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   tc_fence_before();
@@ -225,11 +242,12 @@ k_bsr16_spmm(const __grid_constant__ CUtensorMap tmap_b, const S* __restrict__ p
   if (warp == 4) {
     // ------------------------------------------------------------ producer
     if (lane == 0) {
+      int64_t issued = 0;
       for (int64_t j = 0; j < total; ++j) {
         const int s = static_cast<int>(j % kBsrStages);
         const uint32_t use = static_cast<uint32_t>(j / kBsrStages);
-        if (!mbar_wait(empty0 + 8 * s, (use & 1u) ^ 1u)) {  // slot released by the MMA of block j-S
-          atomicExch(err, 1);
+        if (!mbar_wait(empty0 + 8 * s, (use & 1u) ^ 1u, abort)) {  // slot released by the MMA of block j-S
+          bsr_fail(err, abort);
           break;
         }
         const int64_t blk = b0 + j;
@@ -240,7 +258,13 @@ k_bsr16_spmm(const __grid_constant__ CUtensorMap tmap_b, const S* __restrict__ p
         tma_load_2d(slab, &tmap_b, static_cast<int32_t>(col0), krow, full);
         if (upper) tma_load_2d(slab + 2048, &tmap_b, static_cast<int32_t>(col0 + 64), krow, full);
         bulk_load(base + kSmemBlocks + s * kBlkBytes, packed + blk * 256, kBlkBytes, full);
+        issued = j + 1;
       }
+      // drain: the copies of the last (up to S) blocks issued have landed once
+      // their slot's phase for that use completed (bounded, ignores abort)
+      for (int64_t j = issued > kBsrStages ? issued - kBsrStages : 0; j < issued; ++j)
+        if (!mbar_wait(full0 + 8 * static_cast<int>(j % kBsrStages), static_cast<uint32_t>(j / kBsrStages) & 1u))
+          bsr_fail(err, abort);
     }
   } else if (warp == 5) {
     // ------------------------------------------------------------ MMA issuer
@@ -258,12 +282,12 @@ k_bsr16_spmm(const __grid_constant__ CUtensorMap tmap_b, const S* __restrict__ p
         }
         const bool first = blk == row_begin, last = blk == row_end - 1;
         const int buf = static_cast<int>(rr & 1);
-        if (first && !mbar_wait(acce0 + 8 * buf, static_cast<uint32_t>(((rr >> 1) & 1) ^ 1))) {  // accumulator free
-          atomicExch(err, 1);
+        if (first && !mbar_wait(acce0 + 8 * buf, static_cast<uint32_t>(((rr >> 1) & 1) ^ 1), abort)) {
+          bsr_fail(err, abort);  // accumulator not released
           break;
         }
-        if (!mbar_wait(full0 + 8 * s, use & 1u)) {  // block j landed
-          atomicExch(err, 1);
+        if (!mbar_wait(full0 + 8 * s, use & 1u, abort)) {  // block j landed
+          bsr_fail(err, abort);
           break;
         }
         tc_fence_after();
@@ -277,6 +301,9 @@ k_bsr16_spmm(const __grid_constant__ CUtensorMap tmap_b, const S* __restrict__ p
           ++rr;
         }
       }
+      // drain: every MMA this thread issued has completed once this commit arrives
+      tc_commit(drain);
+      if (!mbar_wait(drain, 0u)) bsr_fail(err, abort);
     }
   } else {
     // ------------------------------------------------------------ epilogue (warps 0-3)
@@ -285,8 +312,8 @@ k_bsr16_spmm(const __grid_constant__ CUtensorMap tmap_b, const S* __restrict__ p
       if (bptr[r] == bptr[r + 1]) continue;
       const int buf = static_cast<int>(rr & 1);
       // warp-uniform outcome: tcgen05.ld below is .sync.aligned
-      if (!__all_sync(0xffffffffu, mbar_wait(accf0 + 8 * buf, static_cast<uint32_t>((rr >> 1) & 1)))) {
-        if (lane == 0) atomicExch(err, 1);
+      if (!__all_sync(0xffffffffu, mbar_wait(accf0 + 8 * buf, static_cast<uint32_t>((rr >> 1) & 1), abort))) {
+        if (lane == 0) bsr_fail(err, abort);
         break;
       }
       tc_fence_after();

@@ -217,6 +217,8 @@ template <> struct YAcc<float> {
   __device__ __forceinline__ void zero() { s = 0.0; }
   __device__ __forceinline__ void add_prod(float a, float b) { s = __fma_rn(double(a), double(b), s); }
   __device__ __forceinline__ void shfl_join(int m) { s = __dadd_rn(s, __shfl_xor_sync(0xffffffffu, s, m)); }
+  __device__ __forceinline__ void shfl_up(int d) { s = __shfl_up_sync(0xffffffffu, s, d); }
+  __device__ __forceinline__ void combine(const YAcc& o) { s = __dadd_rn(s, o.s); }
   __device__ __forceinline__ void store(float* p) const { *reinterpret_cast<double*>(p) = s; }
   __device__ __forceinline__ void add_stored(const float* p) {
     s = __dadd_rn(s, __ldcg(reinterpret_cast<const double*>(p)));
@@ -231,6 +233,11 @@ template <> struct YAcc<double> {
     const double oh = __shfl_xor_sync(0xffffffffu, c.hi, m), ol = __shfl_xor_sync(0xffffffffu, c.lo, m);
     c.add_comp(oh, ol);
   }
+  __device__ __forceinline__ void shfl_up(int d) {
+    c.hi = __shfl_up_sync(0xffffffffu, c.hi, d);
+    c.lo = __shfl_up_sync(0xffffffffu, c.lo, d);
+  }
+  __device__ __forceinline__ void combine(const YAcc& o) { c.add_comp(o.c.hi, o.c.lo); }
   __device__ __forceinline__ void store(double* p) const { p[0] = c.hi; p[1] = c.lo; }
   __device__ __forceinline__ void add_stored(const double* p) { c.add_comp(__ldcg(p), __ldcg(p + 1)); }
   __device__ __forceinline__ double value() const { return c.value(); }
@@ -243,6 +250,13 @@ template <> __device__ __forceinline__ __half ld_once<__half>(const __half* p) {
 template <> __device__ __forceinline__ __nv_bfloat16 ld_once<__nv_bfloat16>(const __nv_bfloat16* p) {
   return __ushort_as_bfloat16(__ldcs(reinterpret_cast<const unsigned short*>(p)));
 }
+
+// Rows of more than this many nonzeros accumulate with Dot2 in the types whose
+// sums run in fp32 (f16, bf16, f32), whatever the plan's flags: their sums are
+// the long ones.  Shorter rows keep the plan's accumulation.
+constexpr int64_t kCompensateAbove = 1024;
+template <int DT, bool COMP>
+constexpr bool kCompLong = !COMP && (DT == FSB_F16 || DT == FSB_BF16 || DT == FSB_F32);
 
 // grid: x = groups of kSpmmWarps units, y = column tiles of 32*V columns.
 // pstride: scratch elements per slot; cps: tickets per slot.
@@ -342,65 +356,119 @@ k_spmm_csr(const typename VT<DT>::Store* __restrict__ data, const int32_t* __res
 
   // ------------------------------------------------------------ long-row chunk
   const int32_t nch = __ldg(&ud->n_chunks), slot = __ldg(&ud->slot);
-  Acc acc;
-  acc.zero();
-  for (int64_t b0 = s0; b0 < s1; b0 += kSpmmBatch) {
-    const int cnt = static_cast<int>(s1 - b0 < kSpmmBatch ? s1 - b0 : int64_t(kSpmmBatch));
-    __syncwarp();
-    for (int k = lane; k < cnt; k += 32) {
-      sh_a[k] = ld_once(data + b0 + k);
-      sh_c[k] = ld_once(col + b0 + k);
-    }
-    __syncwarp();
-    for (int k = 0; k < cnt; k += kSpmmAhead) {
-      S bv[kSpmmAhead][V];
-#pragma unroll
-      for (int u = 0; u < kSpmmAhead; ++u) {
-        const int kk = k + u < cnt ? k + u : k;
-        load_slice<S, V>(B + int64_t(sh_c[kk]) * ldb + c0, k + u < cnt ? nv : 0, bv[u]);
+  // A2: the accumulator of this row's chunks (Dot2 for long rows, see kCompLong)
+  auto run_chunk = [&](auto proto) {
+    using A2 = decltype(proto);
+    A2 acc;
+    acc.zero();
+    for (int64_t b0 = s0; b0 < s1; b0 += kSpmmBatch) {
+      const int cnt = static_cast<int>(s1 - b0 < kSpmmBatch ? s1 - b0 : int64_t(kSpmmBatch));
+      __syncwarp();
+      for (int k = lane; k < cnt; k += 32) {
+        sh_a[k] = ld_once(data + b0 + k);
+        sh_c[k] = ld_once(col + b0 + k);
       }
+      __syncwarp();
+      for (int k = 0; k < cnt; k += kSpmmAhead) {
+        S bv[kSpmmAhead][V];
 #pragma unroll
-      for (int u = 0; u < kSpmmAhead; ++u)
-        if (k + u < cnt) acc.add(sh_a[k + u], bv[u]);
+        for (int u = 0; u < kSpmmAhead; ++u) {
+          const int kk = k + u < cnt ? k + u : k;
+          load_slice<S, V>(B + int64_t(sh_c[kk]) * ldb + c0, k + u < cnt ? nv : 0, bv[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < kSpmmAhead; ++u)
+          if (k + u < cnt) acc.add(sh_a[k + u], bv[u]);
+      }
     }
-  }
-  if (nch == 1) {
-    flush(acc, row);
-    return;
-  }
-  R* part = static_cast<R*>(plan.partials);
-  const int64_t first = int64_t(slot) + (tag + 1);  // slot of the row's first chunk
-  acc.store_partial(part + (int64_t(slot) * pstride + c0) * kER);
-  __threadfence();
-  __syncwarp();
-  int ticket = 0;
-  if (lane == 0) ticket = atomicAdd(plan.counters + first * cps + tile, 1);
-  ticket = __shfl_sync(0xffffffffu, ticket, 0);
-  if (ticket != nch - 1) return;
-  __threadfence();
-  Acc fin;
-  fin.zero();
+    auto put = [&](const A2& a) {
+      if (nv > 0) {
+        S o[V];
+        a.result(o);
+        store_slice(C + int64_t(row) * ldc + c0, nv, o);
+      }
+    };
+    if (nch == 1) {
+      put(acc);
+      return;
+    }
+    R* part = static_cast<R*>(plan.partials);
+    const int64_t first = int64_t(slot) + (tag + 1);  // slot of the row's first chunk
+    acc.store_partial(part + (int64_t(slot) * pstride + c0) * kER);
+    __threadfence();
+    __syncwarp();
+    int ticket = 0;
+    if (lane == 0) ticket = atomicAdd(plan.counters + first * cps + tile, 1);
+    ticket = __shfl_sync(0xffffffffu, ticket, 0);
+    if (ticket != nch - 1) return;
+    __threadfence();
+    A2 fin;
+    fin.zero();
 #pragma unroll 4
-  for (int c = 0; c < nch; ++c) fin.add_partial(part + ((first + c) * pstride + c0) * kER);
-  flush(fin, row);
-  if (lane == 0) plan.counters[first * cps + tile] = 0;  // ready for the next call
+    for (int c = 0; c < nch; ++c) fin.add_partial(part + ((first + c) * pstride + c0) * kER);
+    put(fin);
+    if (lane == 0) plan.counters[first * cps + tile] = 0;  // ready for the next call
+  };
+  if (kCompLong<DT, COMP> && int64_t(nch) * plan.chunk_nnz > kCompensateAbove)
+    run_chunk(SpmmAcc<DT, true, V>());
+  else
+    run_chunk(Acc());
 }
 
 // ---------------------------------------------------------------------------
-// Dense rows made of whole aligned 16-byte slices: teams of T lanes (1 to 32)
-// own 16-byte column slices and whole rows, G = 32 / T teams per warp; rows
-// wider than 512 bytes run 32-lane teams over 512-byte column tiles
-// (grid.y).  One team per warp still beats k_spmm_csr by keeping a row's B
-// slices in flight (1M-row power-law matrix: fp32 N = 128 2.11 ms against
-// 2.24 ms, fp32 N = 256 4.22 against 4.48, fp64 N = 128 4.54 against 10.85).
-//  * row block: team g takes rows g, g+G, ... of the unit; the teams of a warp
-//    walk their rows together up to the longest of them (4 nonzeros ahead,
-//    inactive slots predicated off), so one load instruction moves G rows'
-//    B slices;
-//  * long-row chunk: team g takes nonzeros g, g+G, ...; the team partials are
-//    combined by xor-shuffles over the team index, then the chunk finishes as
-//    in k_spmm_csr (direct store or slot partial + ticket).
+// Dense rows made of whole aligned 16-byte slices: the team kernel.  Teams of
+// T lanes (1 to 32) own the 16-byte slices of a column tile of T * 16 bytes,
+// G = 32 / T teams per warp.  Rows wider than the tile run as several column
+// tiles; the tile is the slowest work dimension, so while one tile is in
+// flight only that tile's slice of B is being gathered, and a slice that fits
+// in L2 is read from HBM about once.
+//
+// Persistent warps stride over the work items of every tile in tile order.
+// An item is either
+//  * a row group: up to kRowUnits consecutive row-block units, split into runs
+//    of adjacent rows.  A run (<= 256 rows, < 512 nonzeros) is staged in the
+//    warp's shared memory and cut by a merge path over its list of row ends
+//    and nonzeros: every team walks the same number of positions whatever the
+//    row lengths, summing nonzeros and writing a row at its end.  A row that
+//    spans teams is finished by a segmented scan over the teams' partial sums
+//    (keys: row indices) in team order;
+//  * a long-row chunk: team g takes nonzeros g, g+G, ...; the team partials
+//    are combined by xor-shuffles over the team index, then the chunk is
+//    stored directly (one-chunk rows) or as a slot partial whose ticket's
+//    last taker adds the partials in chunk order.
+// FUSED: every lane also gathers x[col] beside B's row and sums y = A x for
+// the team's rows (identical sums on the team's lanes; lane 0 writes y).
 // ---------------------------------------------------------------------------
+constexpr int kRowUnits = 4;                            // row-block units per row group
+constexpr int kRowStage = kRowUnits * 2 * kSpmmMaxCap;  // staged nonzeros of a run (< 512)
+constexpr int kRowRows = kRowUnits * kSpmmMaxCap;       // rows of a run (<= 256)
+static_assert(kRowRows <= 256, "run-local row ids are 8-bit");
+static_assert(kSpmmBatch <= kRowStage, "the long-row batch must fit the run staging");
+
+// Per-warp slice: staged values, columns, run-local row ids (8-bit) and row
+// offsets, then (16-byte aligned) one parked accumulator per lane.
+template <typename S>
+constexpr int spmm_team_park_offset() {
+  return (kRowStage * (int(sizeof(S)) + 4 + 1) + (kRowRows + 1) * 4 + 15) & ~15;
+}
+template <int DT, bool COMP>
+constexpr int spmm_team_warp_smem_bytes() {
+  using S = typename VT<DT>::Store;
+  constexpr int V = 16 / int(sizeof(S));
+  return spmm_team_park_offset<S>() + 32 * int(sizeof(SpmmAcc<DT, COMP, V>));
+}
+
+// Resident blocks the register budget is sized for: 3 (85 registers), 2 for
+// complex fp64.
+template <int DT, bool COMP, bool FUSED>
+struct SpmmTeamMinBlocks {
+  static constexpr int value = (DT == FSB_C128) ? 2 : 3;
+};
+
+// B-row slices a team loads ahead of its sums in the row walk
+template <int DT, bool COMP, bool FUSED>
+struct TeamSteps { static constexpr int value = (DT == FSB_F32 && !COMP && !FUSED) ? 8 : 4; };
+
 template <int DT, bool COMP, int V>
 __device__ __forceinline__ void acc_shfl_add(SpmmAcc<DT, COMP, V>& a, int m) {
 #pragma unroll
@@ -417,103 +485,53 @@ __device__ __forceinline__ void acc_shfl_add(SpmmAcc<DT, COMP, V>& a, int m) {
     }
 }
 
-template <int DT, bool COMP, bool FUSED>
-__global__ void __launch_bounds__(kSpmmWarps * 32, SpmmMinBlocks<DT>::value)
-k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __restrict__ col,
-            const int64_t* __restrict__ ptr, const typename VT<DT>::Store* __restrict__ B, int64_t ldb, int64_t n,
-            typename VT<DT>::Store* __restrict__ C, int64_t ldc, fsb_spmv_plan plan, int T, int64_t pstride,
-            int64_t cps, const typename VT<DT>::Store* __restrict__ x, typename VT<DT>::Store* __restrict__ y) {
+// b = the accumulator of the lane `delta` below (the lane itself where there is none)
+template <int DT, bool COMP, int V>
+__device__ __forceinline__ void acc_shfl_up(const SpmmAcc<DT, COMP, V>& a, SpmmAcc<DT, COMP, V>& b, int delta) {
+#pragma unroll
+  for (int c = 0; c < SpmmAcc<DT, COMP, V>::kNC; ++c)
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      b.s[c][j].hi = __shfl_up_sync(0xffffffffu, a.s[c][j].hi, delta);
+      if constexpr (COMP) b.s[c][j].lo = __shfl_up_sync(0xffffffffu, a.s[c][j].lo, delta);
+    }
+}
+
+template <int DT, bool COMP, int V>
+__device__ __forceinline__ void acc_combine(SpmmAcc<DT, COMP, V>& a, const SpmmAcc<DT, COMP, V>& b) {
+#pragma unroll
+  for (int c = 0; c < SpmmAcc<DT, COMP, V>::kNC; ++c)
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      if constexpr (COMP) a.s[c][j].add_comp(b.s[c][j].hi, b.s[c][j].lo);
+      else a.s[c][j].add(b.s[c][j].hi);
+    }
+}
+
+// One long-row chunk of the team kernel: team g takes nonzeros g, g+G, ...;
+// the team partials are combined by xor-shuffles over the team index, then
+// the chunk is stored directly (one-chunk rows) or as a slot partial whose
+// ticket's last taker adds the partials in chunk order.  ACOMP selects the
+// accumulator (Dot2 or plain).
+template <int DT, bool ACOMP, bool FUSED>
+__device__ __forceinline__ void team_chunk(const typename VT<DT>::Store* __restrict__ data,
+                                           const int32_t* __restrict__ col,
+                                           const typename VT<DT>::Store* __restrict__ B, int64_t ldb, int64_t n,
+                                           typename VT<DT>::Store* __restrict__ C, int64_t ldc,
+                                           const fsb_spmv_plan& plan, const fsb_spmv_unit* ud, int T, int64_t tile,
+                                           int64_t c0, int nv, int64_t pstride, int64_t cps,
+                                           const typename VT<DT>::Store* __restrict__ x,
+                                           typename VT<DT>::Store* __restrict__ y, typename VT<DT>::Store* sh_a,
+                                           int32_t* sh_c) {
   using S = typename VT<DT>::Store;
   using R = typename VT<DT>::Real;
   constexpr int V = 16 / int(sizeof(S));
-  using Acc = SpmmAcc<DT, COMP, V>;
+  using Acc = SpmmAcc<DT, ACOMP, V>;
   constexpr int kER = Acc::kNC * 2;
-  constexpr int kTA = FUSED ? 4 : TeamAhead<DT>::value;
-  // FUSED: the team's lanes also sum y = A x for its rows (item q * T + tl of
-  // each group of loads to lane tl), gathering x[col] beside the B row of the
-  // same nonzero.
-
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int64_t unit = int64_t(blockIdx.x) * kSpmmWarps + warp;
-  if (unit >= plan.n_units) return;  // whole warp leaves together
-  const int G = 32 / T, team = lane / T, tl = lane % T;
-  const int64_t c0 = int64_t(blockIdx.y) * (T * V) + int64_t(tl) * V;  // rows wider than 32 lanes: 512-byte tiles
-  const int nv = c0 + V <= n ? V : 0;  // n is a multiple of V
-
-  unsigned char* wbase = smem_raw + warp * spmm_warp_smem_bytes<S>();
-  S* sh_a = reinterpret_cast<S*>(wbase);
-  int32_t* sh_c = reinterpret_cast<int32_t*>(wbase + kSpmmBatch * sizeof(S));
-  int32_t* sh_off = sh_c + kSpmmBatch;
-
-  const fsb_spmv_unit* ud = plan.units + unit;
+  const int lane = threadIdx.x & 31;
+  const int G = 32 / T, team = lane / T;
   const int64_t s0 = __ldg(&ud->nnz_begin), s1 = __ldg(&ud->nnz_end);
   const int32_t row = __ldg(&ud->row), tag = __ldg(&ud->tag);
-
-  if (tag >= 0) {
-    // ------------------------------------------------------------ row block
-    const int nr = tag - row;
-    const int cnt = static_cast<int>(s1 - s0);
-    for (int i = lane; i <= nr; i += 32) sh_off[i] = static_cast<int32_t>(__ldg(ptr + row + i) - s0);
-    for (int k = lane; k < cnt; k += 32) {
-      sh_a[k] = ld_once(data + s0 + k);
-      sh_c[k] = ld_once(col + s0 + k);
-    }
-    __syncwarp();
-    for (int i0 = 0; i0 < nr; i0 += G) {
-      const int i = i0 + team;
-      const bool has = i < nr;
-      const int b = has ? sh_off[i] : 0;
-      const int len = has ? sh_off[i + 1] - b : 0;
-      int maxlen = len;
-      for (int m = T; m < 32; m <<= 1) maxlen = max(maxlen, __shfl_xor_sync(0xffffffffu, maxlen, m));
-      Acc acc;
-      acc.zero();
-      YAcc<R> yacc;
-      yacc.zero();
-      for (int k = 0; k < maxlen; k += kTA) {
-        S bv[kTA][V];
-        S xv[kTA];
-#pragma unroll
-        for (int u = 0; u < kTA; ++u) {
-          const bool ok = k + u < len;
-          load_slice<S, V>(B + int64_t(sh_c[ok ? b + k + u : 0]) * ldb + c0, ok ? nv : 0, bv[u]);
-        }
-        if constexpr (FUSED) {
-          // item q * T + tl of this group goes to lane tl: every lane works at once
-#pragma unroll
-          for (int q = 0; q < kTA; ++q) {
-            const int u = q * T + tl;
-            if (q * T < kTA && u < kTA && k + u < len) xv[q] = ld_gather(x + sh_c[b + k + u]);
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < kTA; ++u)
-          if (k + u < len) acc.add(sh_a[b + k + u], bv[u]);
-        if constexpr (FUSED) {
-#pragma unroll
-          for (int q = 0; q < kTA; ++q) {
-            const int u = q * T + tl;
-            if (q * T < kTA && u < kTA && k + u < len)
-              yacc.add_prod(to_real(sh_a[b + k + u]), to_real(xv[q]));
-          }
-        }
-      }
-      if (has && nv > 0) {
-        S o[V];
-        acc.result(o);
-        store_slice(C + (int64_t(row) + i) * ldc + c0, nv, o);
-      }
-      if constexpr (FUSED) {
-        // join the y terms spread over the team's lanes
-        for (int m = 1; m < T; m <<= 1) yacc.shfl_join(m);
-        if (has && tl == 0) put_y(y[int64_t(row) + i], yacc.value());
-      }
-    }
-    return;
-  }
-
-  // ------------------------------------------------------------ long-row chunk
   const int32_t nch = __ldg(&ud->n_chunks), slot = __ldg(&ud->slot);
   Acc acc;
   acc.zero();
@@ -531,9 +549,9 @@ k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __re
       S bv[kSpmmAhead][V];
       S xv[kSpmmAhead];
 #pragma unroll
-      for (int u = 0; u < kSpmmAhead; ++u) {
-        const int kk = k + u * G + team;
-        load_slice<S, V>(B + int64_t(sh_c[kk < cnt ? kk : 0]) * ldb + c0, kk < cnt ? nv : 0, bv[u]);
+      for (int q = 0; q < kSpmmAhead; ++q) {
+        const int kk = k + q * G + team;
+        load_slice<S, V>(B + int64_t(sh_c[kk < cnt ? kk : 0]) * ldb + c0, kk < cnt ? nv : 0, bv[q]);
       }
       if constexpr (FUSED) {
         // the y terms of these kSpmmAhead * G items, one per lane in order
@@ -544,9 +562,9 @@ k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __re
         }
       }
 #pragma unroll
-      for (int u = 0; u < kSpmmAhead; ++u) {
-        const int kk = k + u * G + team;
-        if (kk < cnt) acc.add(sh_a[kk], bv[u]);
+      for (int q = 0; q < kSpmmAhead; ++q) {
+        const int kk = k + q * G + team;
+        if (kk < cnt) acc.add(sh_a[kk], bv[q]);
       }
       if constexpr (FUSED) {
 #pragma unroll
@@ -569,42 +587,258 @@ k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __re
       store_slice(C + int64_t(row) * ldc + c0, nv, o);
     }
     if constexpr (FUSED)
-      if (lane == 0) put_y(y[row], yacc.value());
+      if (lane == 0 && tile == 0) put_y(y[row], yacc.value());
     return;
   }
   R* part = static_cast<R*>(plan.partials);
-  const int64_t first = int64_t(slot) + (tag + 1);
+  const int64_t first = int64_t(slot) + (tag + 1);  // slot of the row's first chunk
   if (team == 0) acc.store_partial(part + (int64_t(slot) * pstride + c0) * kER);
   if constexpr (FUSED) {
     // y's partial sits in the slot's column n (n < pstride for the fused path)
-    if (lane == 0) yacc.store(part + (int64_t(slot) * pstride + n) * kER);
+    if (lane == 0 && tile == 0) yacc.store(part + (int64_t(slot) * pstride + n) * kER);
   }
   __threadfence();
   __syncwarp();
   int ticket = 0;
-  if (lane == 0) ticket = atomicAdd(plan.counters + first * cps + blockIdx.y, 1);
+  if (lane == 0) ticket = atomicAdd(plan.counters + first * cps + tile, 1);
   ticket = __shfl_sync(0xffffffffu, ticket, 0);
   if (ticket != nch - 1) return;
   __threadfence();
-  if (team != 0) return;
-  Acc fin;
-  fin.zero();
+  if (team == 0) {
+    Acc fin;
+    fin.zero();
 #pragma unroll 4
-  for (int c = 0; c < nch; ++c) fin.add_partial(part + ((first + c) * pstride + c0) * kER);
-  if (nv > 0) {
-    S o[V];
-    fin.result(o);
-    store_slice(C + int64_t(row) * ldc + c0, nv, o);
-  }
-  if constexpr (FUSED) {
-    if (lane == 0) {
-      YAcc<R> fy;
-      fy.zero();
-      for (int c = 0; c < nch; ++c) fy.add_stored(part + ((first + c) * pstride + n) * kER);
-      put_y(y[row], fy.value());
+    for (int c = 0; c < nch; ++c) fin.add_partial(part + ((first + c) * pstride + c0) * kER);
+    if (nv > 0) {
+      S o[V];
+      fin.result(o);
+      store_slice(C + int64_t(row) * ldc + c0, nv, o);
     }
+    if constexpr (FUSED) {
+      if (lane == 0 && tile == 0) {
+        YAcc<R> fy;
+        fy.zero();
+        for (int c = 0; c < nch; ++c) fy.add_stored(part + ((first + c) * pstride + n) * kER);
+        put_y(y[row], fy.value());
+      }
+    }
+    if (lane == 0) plan.counters[first * cps + tile] = 0;  // ready for the next call
   }
-  if (lane == 0) plan.counters[first * cps + blockIdx.y] = 0;  // ready for the next call
+}
+
+template <int DT, bool COMP, bool FUSED>
+__global__ void __launch_bounds__(kSpmmWarps * 32, SpmmTeamMinBlocks<DT, COMP, FUSED>::value)
+k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __restrict__ col,
+            const int64_t* __restrict__ ptr, const typename VT<DT>::Store* __restrict__ B, int64_t ldb, int64_t n,
+            typename VT<DT>::Store* __restrict__ C, int64_t ldc, fsb_spmv_plan plan, int T, int64_t tiles,
+            int64_t pstride, int64_t cps, const typename VT<DT>::Store* __restrict__ x,
+            typename VT<DT>::Store* __restrict__ y) {
+  using S = typename VT<DT>::Store;
+  using R = typename VT<DT>::Real;
+  constexpr int V = 16 / int(sizeof(S));
+  using Acc = SpmmAcc<DT, COMP, V>;
+  constexpr int kP = TeamSteps<DT, COMP, FUSED>::value;
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int G = 32 / T, team = lane / T, tl = lane % T;
+  unsigned char* wbase = smem_raw + warp * spmm_team_warp_smem_bytes<DT, COMP>();
+  S* sh_a = reinterpret_cast<S*>(wbase);
+  int32_t* sh_c = reinterpret_cast<int32_t*>(wbase + kRowStage * sizeof(S));
+  int32_t* sh_off = sh_c + kRowStage;
+  uint8_t* sh_rid = reinterpret_cast<uint8_t*>(sh_off + kRowRows + 1);
+  Acc* sh_park = reinterpret_cast<Acc*>(wbase + spmm_team_park_offset<S>()) + lane;
+
+  const int64_t nb = plan.n_block_units;
+  const uint32_t n_groups = static_cast<uint32_t>(ceil_div(nb, kRowUnits));
+  const uint32_t n_items = n_groups + static_cast<uint32_t>(plan.n_units - nb);
+  const uint32_t total = n_items * static_cast<uint32_t>(tiles);
+  const uint32_t nwarps = gridDim.x * kSpmmWarps;
+
+  for (uint32_t it = blockIdx.x * kSpmmWarps + warp; it < total; it += nwarps) {
+    const uint32_t tile = it / n_items, item = it - tile * n_items;
+    const int64_t c0 = int64_t(tile) * (int64_t(T) * V) + int64_t(tl) * V;  // this lane's first column
+    const int nv = c0 + V <= n ? V : 0;                       // n is a multiple of V
+    __syncwarp();  // the staging slice of the previous item is free
+
+    if (item < n_groups) {
+      // ---------------------------------------------------------- row group
+      // lanes 0 .. kRowUnits-1 hold the group's unit descriptors
+      const int64_t ua = int64_t(item) * kRowUnits;
+      const int nu = static_cast<int>(nb - ua < kRowUnits ? nb - ua : int64_t(kRowUnits));
+      int64_t d_s0 = 0, d_s1 = 0;
+      int32_t d_row = 0, d_tag = 0;
+      if (lane < nu) {
+        const int4* p = reinterpret_cast<const int4*>(plan.units + ua + lane);
+        const int4 a = __ldg(p), b = __ldg(p + 1);
+        d_s0 = (int64_t)(uint32_t)a.x | ((int64_t)a.y << 32);
+        d_s1 = (int64_t)(uint32_t)a.z | ((int64_t)a.w << 32);
+        d_row = b.x;
+        d_tag = b.y;
+      }
+      int u = 0;
+      while (u < nu) {
+        // the run: units u .. v-1 whose rows join up (a long row between two
+        // units, listed among the chunks, breaks the run)
+        const int32_t r0 = __shfl_sync(0xffffffffu, d_row, u);
+        const int64_t s0 = __shfl_sync(0xffffffffu, d_s0, u);
+        int32_t r1 = __shfl_sync(0xffffffffu, d_tag, u);
+        int64_t s1 = __shfl_sync(0xffffffffu, d_s1, u);
+        int v = u + 1;
+        for (; v < nu; ++v) {
+          if (__shfl_sync(0xffffffffu, d_row, v) != r1) break;
+          r1 = __shfl_sync(0xffffffffu, d_tag, v);
+          s1 = __shfl_sync(0xffffffffu, d_s1, v);
+        }
+        u = v;
+        const int nr = r1 - r0;
+        const int cnt = static_cast<int>(s1 - s0);
+        __syncwarp();
+        for (int i = lane; i <= nr; i += 32) sh_off[i] = static_cast<int32_t>(__ldg(ptr + r0 + i) - s0);
+        for (int k = lane; k < cnt; k += 32) {
+          sh_a[k] = ld_once(data + s0 + k);
+          sh_c[k] = ld_once(col + s0 + k);
+        }
+        __syncwarp();
+        // run-local row of every nonzero; empty rows get zero slices (one team each)
+        for (int i0 = 0; i0 < nr; i0 += 32) {
+          const int i = i0 + lane;
+          bool empty = false;
+          if (i < nr) {
+            const int b = sh_off[i], e = sh_off[i + 1];
+            for (int k = b; k < e; ++k) sh_rid[k] = static_cast<uint8_t>(i);
+            empty = b == e;
+          }
+          unsigned m = __ballot_sync(0xffffffffu, empty);
+          for (int q = 0; m; ++q) {
+            const int b = __ffs(m) - 1;
+            m &= m - 1;
+            if (q % G == team) {
+              if (nv > 0) {
+                Acc z;
+                z.zero();
+                S o[V];
+                z.result(o);
+                store_slice(C + (int64_t(r0) + i0 + b) * ldc + c0, nv, o);
+              }
+              if constexpr (FUSED)
+                if (tl == 0 && tile == 0) put_y(y[int64_t(r0) + i0 + b], 0.0f);
+            }
+          }
+        }
+        __syncwarp();
+
+        // team g sums nonzeros [jb, je) of the run: an equal share whatever the
+        // row lengths.  A row is written by the team holding its last nonzero;
+        // the partials of a row spanning several teams are totalled by a
+        // segmented scan over the teams (keys: run-local rows).
+        const int per = (cnt + G - 1) / G;
+        const int jb = min(team * per, cnt), je = min(jb + per, cnt);
+        Acc acc;
+        acc.zero();
+        YAcc<R> yacc, ypark;
+        yacc.zero();
+        ypark.zero();
+        int cur = jb < je ? sh_rid[jb] : 0;
+        bool open_start = jb < je && sh_off[cur] < jb;  // row cur began in an earlier team
+        int park_row = -1;
+        auto put_row = [&](const Acc& a, const YAcc<R>& ya, int r) {
+          if (nv > 0) {
+            S o[V];
+            a.result(o);
+            store_slice(C + (int64_t(r0) + r) * ldc + c0, nv, o);
+          }
+          if constexpr (FUSED)
+            if (tl == 0 && tile == 0) put_y(y[int64_t(r0) + r], ya.value());
+        };
+        for (int j0 = jb; j0 < je; j0 += kP) {
+          S bv[kP][V];
+          S xv[kP];
+#pragma unroll
+          for (int q = 0; q < kP; ++q) {  // past je: the last nonzero again, loaded and not summed
+            const int j = j0 + q < je ? j0 + q : je - 1;
+            load_slice<S, V>(B + int64_t(sh_c[j]) * ldb + c0, nv, bv[q]);
+            if constexpr (FUSED) xv[q] = ld_gather(x + sh_c[j]);
+          }
+#pragma unroll
+          for (int q = 0; q < kP; ++q) {
+            const int j = j0 + q;
+            if (j < je) {
+              const int r = sh_rid[j];
+              if (r != cur) {  // row cur ended before nonzero j
+                if (open_start) {
+                  *sh_park = acc;  // finished after the scan
+                  ypark = yacc;
+                  park_row = cur;
+                  open_start = false;
+                } else {
+                  put_row(acc, yacc, cur);
+                }
+                acc.zero();
+                yacc.zero();
+                cur = r;
+              }
+              const S a = sh_a[j];
+              acc.add(a, bv[q]);
+              if constexpr (FUSED) yacc.add_prod(to_real(a), to_real(xv[q]));
+            }
+          }
+        }
+        const bool open_end = jb < je && sh_off[cur + 1] > je;  // row cur goes on in later teams
+        // inclusive segmented scan of the open-ended partials over the teams
+        const int key = open_end ? cur : -1;
+        Acc sc = acc;
+        YAcc<R> ysc = yacc;
+        if (!open_end) {
+          sc.zero();
+          ysc.zero();
+        }
+        for (int o = 1; o < G; o <<= 1) {
+          Acc other;
+          acc_shfl_up(sc, other, o * T);
+          YAcc<R> oy = ysc;
+          if constexpr (FUSED) oy.shfl_up(o * T);
+          const int okey = __shfl_up_sync(0xffffffffu, key, o * T);
+          if (team >= o && key >= 0 && okey == key) {
+            acc_combine(sc, other);
+            if constexpr (FUSED) ysc.combine(oy);
+          }
+        }
+        Acc carry;
+        acc_shfl_up(sc, carry, T);
+        YAcc<R> ycarry = ysc;
+        if constexpr (FUSED) ycarry.shfl_up(T);
+        // the partials of earlier teams belong to the row this team began inside
+        if (park_row >= 0) {
+          Acc f = *sh_park;
+          acc_combine(f, carry);
+          if constexpr (FUSED) ypark.combine(ycarry);
+          put_row(f, ypark, park_row);
+        }
+        if (jb < je && !open_end) {
+          if (open_start) {  // this team holds the end of a row begun before it
+            acc_combine(acc, carry);
+            if constexpr (FUSED) yacc.combine(ycarry);
+          }
+          put_row(acc, yacc, cur);
+        }
+        __syncwarp();  // the staging slice is rewritten by the next run
+      }
+      continue;
+    }
+
+    // ------------------------------------------------------------ long-row chunk
+    const fsb_spmv_unit* ud = plan.units + nb + (item - n_groups);
+    const int32_t nch = __ldg(&ud->n_chunks);
+    // rows of more than kCompensateAbove nonzeros sum with Dot2 (compensated)
+    // accumulators in the fp32-accumulated types, partials and all
+    if (kCompLong<DT, COMP> && int64_t(nch) * plan.chunk_nnz > kCompensateAbove)
+      team_chunk<DT, COMP || kCompLong<DT, COMP>, FUSED>(data, col, B, ldb, n, C, ldc, plan, ud, T, tile, c0, nv,
+                                                         pstride, cps, x, y, sh_a, sh_c);
+    else
+      team_chunk<DT, COMP, FUSED>(data, col, B, ldb, n, C, ldc, plan, ud, T, tile, c0, nv, pstride, cps, x, y, sh_a,
+                                  sh_c);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -805,62 +1039,70 @@ k_spmm_bwd(const typename VT<DT>::Store* __restrict__ vals, const int32_t* __res
 #pragma unroll
     for (int j = 0; j < V; ++j) xf[j] = to_real(xs[j]);
   }
-  Acc acc;
-  acc.zero();
-  for (int64_t b0 = s0; b0 < s1; b0 += kSpmmBatch) {
-    const int cnt = static_cast<int>(s1 - b0 < kSpmmBatch ? s1 - b0 : int64_t(kSpmmBatch));
-    __syncwarp();
-    stage(b0, cnt);
-    __syncwarp();
-    for (int k = 0; k < cnt; k += kA * G) {
-      S bv[kA][V];
+  // A2: the accumulator of this row's chunks (Dot2 for long rows, see kCompLong)
+  auto run_chunk = [&](auto proto) {
+    using A2 = decltype(proto);
+    A2 acc;
+    acc.zero();
+    for (int64_t b0 = s0; b0 < s1; b0 += kSpmmBatch) {
+      const int cnt = static_cast<int>(s1 - b0 < kSpmmBatch ? s1 - b0 : int64_t(kSpmmBatch));
+      __syncwarp();
+      stage(b0, cnt);
+      __syncwarp();
+      for (int k = 0; k < cnt; k += kA * G) {
+        S bv[kA][V];
 #pragma unroll
-      for (int u = 0; u < kA; ++u) {
-        const int kk = k + u * G + team;
-        load_slice<S, V>(dY + int64_t(sh_c[kk < cnt ? kk : 0]) * lddy + c0, kk < cnt ? nv : 0, bv[u]);
-      }
+        for (int u = 0; u < kA; ++u) {
+          const int kk = k + u * G + team;
+          load_slice<S, V>(dY + int64_t(sh_c[kk < cnt ? kk : 0]) * lddy + c0, kk < cnt ? nv : 0, bv[u]);
+        }
 #pragma unroll
-      for (int u = 0; u < kA; ++u) {
-        const int kk = k + u * G + team;
-        if (kk < cnt) acc.add(sh_a[kk], bv[u]);
-      }
-      if constexpr (DV) {
-        R d[kA];
-        bwd_dots<S, R, kA, V>(bv, xf, d);
-        bwd_put_dots<S, R, kA>(d, k + team, G, cnt, T, tl, sh_p, dvals);
+        for (int u = 0; u < kA; ++u) {
+          const int kk = k + u * G + team;
+          if (kk < cnt) acc.add(sh_a[kk], bv[u]);
+        }
+        if constexpr (DV) {
+          R d[kA];
+          bwd_dots<S, R, kA, V>(bv, xf, d);
+          bwd_put_dots<S, R, kA>(d, k + team, G, cnt, T, tl, sh_p, dvals);
+        }
       }
     }
-  }
-  for (int m = T; m < 32; m <<= 1) acc_shfl_add(acc, m);  // every team now holds the chunk's sum
-  if (nch == 1) {
-    if (team == 0 && nv > 0) {
+    for (int m = T; m < 32; m <<= 1) acc_shfl_add(acc, m);  // every team now holds the chunk's sum
+    if (nch == 1) {
+      if (team == 0 && nv > 0) {
+        S o[V];
+        acc.result(o);
+        store_slice<S, V, true>(dX + int64_t(row) * lddx + c0, nv, o);
+      }
+      return;
+    }
+    R* part = static_cast<R*>(plan.partials);
+    const int64_t first = int64_t(slot) + (tag + 1);
+    if (team == 0) acc.store_partial(part + (int64_t(slot) * pstride + c0) * kER);
+    __threadfence();
+    __syncwarp();
+    int ticket = 0;
+    if (lane == 0) ticket = atomicAdd(plan.counters + first * cps, 1);
+    ticket = __shfl_sync(0xffffffffu, ticket, 0);
+    if (ticket != nch - 1) return;
+    __threadfence();
+    if (team != 0) return;
+    A2 fin;
+    fin.zero();
+#pragma unroll 4
+    for (int c = 0; c < nch; ++c) fin.add_partial(part + ((first + c) * pstride + c0) * kER);
+    if (nv > 0) {
       S o[V];
-      acc.result(o);
+      fin.result(o);
       store_slice<S, V, true>(dX + int64_t(row) * lddx + c0, nv, o);
     }
-    return;
-  }
-  R* part = static_cast<R*>(plan.partials);
-  const int64_t first = int64_t(slot) + (tag + 1);
-  if (team == 0) acc.store_partial(part + (int64_t(slot) * pstride + c0) * kER);
-  __threadfence();
-  __syncwarp();
-  int ticket = 0;
-  if (lane == 0) ticket = atomicAdd(plan.counters + first * cps, 1);
-  ticket = __shfl_sync(0xffffffffu, ticket, 0);
-  if (ticket != nch - 1) return;
-  __threadfence();
-  if (team != 0) return;
-  Acc fin;
-  fin.zero();
-#pragma unroll 4
-  for (int c = 0; c < nch; ++c) fin.add_partial(part + ((first + c) * pstride + c0) * kER);
-  if (nv > 0) {
-    S o[V];
-    fin.result(o);
-    store_slice<S, V, true>(dX + int64_t(row) * lddx + c0, nv, o);
-  }
-  if (lane == 0) plan.counters[first * cps] = 0;  // ready for the next call
+    if (lane == 0) plan.counters[first * cps] = 0;  // ready for the next call
+  };
+  if (kCompLong<DT, false> && int64_t(nch) * plan.chunk_nnz > kCompensateAbove)
+    run_chunk(SpmmAcc<DT, true, V>());
+  else
+    run_chunk(Acc());
 }
 
 }  // namespace
@@ -877,8 +1119,63 @@ inline int64_t spmm_real_bytes(int dtype) {
   }
 }
 
+inline int64_t spmm_elem_bytes(int dtype) {
+  switch (dtype) {
+    case FSB_F16: case FSB_BF16: return 2;
+    case FSB_F32: return 4;
+    case FSB_F64: case FSB_C64: return 8;
+    case FSB_C128: return 16;
+    default: return -1;
+  }
+}
+
 inline int64_t spmm_pstride(int64_t n) { return ceil_div(n, 256) * 256; }
-inline int64_t spmm_cps(int64_t n) { return n > 32 ? ceil_div(n, 32) : 1; }
+// Tickets per slot: one per column tile.  The narrowest tile of any kernel is
+// one 16-byte slice, so ceil(n * elem / 16) covers every tiling.
+inline int64_t spmm_cps_bytes(int64_t n, int64_t elem) { return n > 0 ? ceil_div(n * elem, 16) : 1; }
+template <int DT>
+inline int64_t spmm_cps(int64_t n) { return spmm_cps_bytes(n, sizeof(typename VT<DT>::Store)); }
+
+// Column tile of the team kernel, in bytes (a power of two, 16 .. 512).  The
+// default is the whole row (rounded up to a power of two of 16-byte slices) up
+// to 512 bytes, halved down to 64 bytes while the tile's slice of B, n_cols x
+// tile bytes, exceeds kSpmmL2Slice: a slice that fits in L2 is gathered from
+// L2 after its first read, which pays for re-reading A once per tile.  A
+// positive `hint` (fsb_spmv_plan.tile_bytes) replaces the default.
+constexpr int64_t kSpmmL2Slice = int64_t(80) << 20;
+inline int spmm_team_tile_bytes(int64_t row_bytes, int64_t n_cols, int32_t hint) {
+  int w = 16;
+  while (w < row_bytes && w < 512) w *= 2;
+  if (hint > 0) {
+    int h = 16;
+    while (h < hint && h < 512) h *= 2;
+    return h < w ? h : w;
+  }
+  while (w > 64 && n_cols * w > kSpmmL2Slice) w /= 2;
+  return w;
+}
+
+// Resident blocks per SM of a kernel at this block size and shared memory,
+// looked up once per kernel (and device ordinal) and kept.
+template <typename K>
+int64_t resident_blocks(K kern, int threads, size_t smem) {
+  static int cached[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+    (void)cudaGetLastError();
+    return 148;
+  }
+  if (cached[dev] == 0) {
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || per_sm < 1 || sms < 1) {
+      (void)cudaGetLastError();
+      return 148;
+    }
+    cached[dev] = per_sm * sms;
+  }
+  return cached[dev];
+}
 
 template <int DT, int V, bool COMP>
 int spmm_launch_v(const void* data, const int32_t* idx, const int64_t* ptr, const void* B, int64_t ldb, int64_t n,
@@ -891,7 +1188,7 @@ int spmm_launch_v(const void* data, const int32_t* idx, const int64_t* ptr, cons
   dim3 grid((unsigned)blocks, (unsigned)tiles);
   k_spmm_csr<DT, V, COMP><<<grid, kSpmmWarps * 32, smem, st>>>(
       static_cast<const S*>(data), idx, ptr, static_cast<const S*>(B), ldb, n, static_cast<S*>(C), ldc, plan,
-      spmm_pstride(n), spmm_cps(n));
+      spmm_pstride(n), spmm_cps<DT>(n));
   FSB_LAUNCH_CHECK();
   return FSB_OK;
 }
@@ -913,16 +1210,33 @@ int spmm_pick_v(const void* B, int64_t ldb, const void* C, int64_t ldc, int64_t 
   return v;
 }
 
+// The team kernel, persistent: at most the resident blocks, each warp striding
+// over the work items of every tile (tile bytes = T * 16).
 template <int DT, bool COMP, bool FUSED = false>
 int spmm_launch_team(const void* data, const int32_t* idx, const int64_t* ptr, const void* B, int64_t ldb, int64_t n,
-                     void* C, int64_t ldc, const fsb_spmv_plan& plan, int T, cudaStream_t st,
-                     const void* x = nullptr, void* y = nullptr, int64_t tiles = 1) {
+                     void* C, int64_t ldc, const fsb_spmv_plan& plan, int T, int64_t tiles, cudaStream_t st,
+                     const void* x = nullptr, void* y = nullptr) {
   using S = typename VT<DT>::Store;
-  const int64_t blocks = ceil_div(plan.n_units, kSpmmWarps);
-  const size_t smem = size_t(spmm_warp_smem_bytes<S>()) * kSpmmWarps;
-  k_spmm_team<DT, COMP, FUSED><<<dim3((unsigned)blocks, (unsigned)tiles), kSpmmWarps * 32, smem, st>>>(
+  const size_t smem = size_t(spmm_team_warp_smem_bytes<DT, COMP>()) * kSpmmWarps;
+  auto kern = k_spmm_team<DT, COMP, FUSED>;
+  static bool attr_set = false;  // per instantiation; the attribute is per function
+  if (!attr_set) {
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+      (void)cudaGetLastError();
+      return FSB_ERR_CUDA;
+    }
+    attr_set = true;
+  }
+  const int64_t nb = plan.n_block_units;
+  const int64_t items = (ceil_div(nb, kRowUnits) + (plan.n_units - nb)) * tiles;
+  int64_t blocks = ceil_div(items, kSpmmWarps);
+  const int64_t resident = resident_blocks(kern, kSpmmWarps * 32, smem);
+  if (blocks > resident) blocks = resident;
+  if (blocks < 1) return FSB_OK;
+  kern<<<(unsigned)blocks, kSpmmWarps * 32, smem, st>>>(
       static_cast<const S*>(data), idx, ptr, static_cast<const S*>(B), ldb, n, static_cast<S*>(C), ldc, plan, T,
-      spmm_pstride(n), spmm_cps(n), static_cast<const S*>(x), static_cast<S*>(y));
+      tiles, spmm_pstride(n), spmm_cps<DT>(n), static_cast<const S*>(x), static_cast<S*>(y));
   FSB_LAUNCH_CHECK();
   return FSB_OK;
 }
@@ -945,8 +1259,8 @@ int spmm_spmv_fused(const void* data, const int32_t* idx, const int64_t* ptr, co
     int T = 1;
     while (int64_t(T) * kVmax < n) T *= 2;
     if (plan.flags & FSB_SPMM_COMPENSATED)
-      return spmm_launch_team<DT, true, true>(data, idx, ptr, B, ldb, n, C, ldc, plan, T, st, x, y);
-    return spmm_launch_team<DT, false, true>(data, idx, ptr, B, ldb, n, C, ldc, plan, T, st, x, y);
+      return spmm_launch_team<DT, true, true>(data, idx, ptr, B, ldb, n, C, ldc, plan, T, 1, st, x, y);
+    return spmm_launch_team<DT, false, true>(data, idx, ptr, B, ldb, n, C, ldc, plan, T, 1, st, x, y);
   }
 }
 
@@ -975,11 +1289,11 @@ int spmm_backward(const void* vals, const int32_t* perm, const int32_t* idx, con
     if (dvals) {
       k_spmm_bwd<DT, true><<<(unsigned)blocks, kSpmmWarps * 32, smem, st>>>(
           v, perm, idx, ptr, static_cast<const S*>(dY), lddy, n, static_cast<const S*>(X), ldx,
-          static_cast<S*>(dX), lddx, static_cast<S*>(dvals), plan, T, spmm_pstride(n), spmm_cps(n));
+          static_cast<S*>(dX), lddx, static_cast<S*>(dvals), plan, T, spmm_pstride(n), spmm_cps<DT>(n));
     } else {
       k_spmm_bwd<DT, false><<<(unsigned)blocks, kSpmmWarps * 32, smem, st>>>(
           v, perm, idx, ptr, static_cast<const S*>(dY), lddy, n, nullptr, 0, static_cast<S*>(dX), lddx, nullptr,
-          plan, T, spmm_pstride(n), spmm_cps(n));
+          plan, T, spmm_pstride(n), spmm_cps<DT>(n));
     }
     FSB_LAUNCH_CHECK();
     return FSB_OK;
@@ -988,21 +1302,18 @@ int spmm_backward(const void* vals, const int32_t* perm, const int32_t* idx, con
 
 template <int DT, bool COMP>
 int spmm_dispatch(const void* data, const int32_t* idx, const int64_t* ptr, const void* B, int64_t ldb, int64_t n,
-                  void* C, int64_t ldc, const fsb_spmv_plan& plan, cudaStream_t st) {
+                  int64_t n_cols, void* C, int64_t ldc, const fsb_spmv_plan& plan, cudaStream_t st) {
   using S = typename VT<DT>::Store;
   constexpr int kVmax = 16 / int(sizeof(S));
-  // narrow rows with whole, aligned 16-byte slices: teams of T lanes own rows
-  if (n * int64_t(sizeof(S)) <= 512 && n % kVmax == 0 && ldb % kVmax == 0 && ldc % kVmax == 0 &&
-      reinterpret_cast<uintptr_t>(B) % 16 == 0 && reinterpret_cast<uintptr_t>(C) % 16 == 0) {
-    int T = 1;
-    while (int64_t(T) * kVmax < n) T *= 2;
-    return spmm_launch_team<DT, COMP>(data, idx, ptr, B, ldb, n, C, ldc, plan, T, st);
-  }
-  // wider rows of whole aligned slices: 32-lane teams over 512-byte column tiles
+  // rows of whole, aligned 16-byte slices: teams of T lanes over column tiles
+  // of T * 16 bytes (spmm_team_tile_bytes)
   if (n % kVmax == 0 && ldb % kVmax == 0 && ldc % kVmax == 0 && reinterpret_cast<uintptr_t>(B) % 16 == 0 &&
-      reinterpret_cast<uintptr_t>(C) % 16 == 0 && ceil_div(n, int64_t(32) * kVmax) <= 65535)
-    return spmm_launch_team<DT, COMP>(data, idx, ptr, B, ldb, n, C, ldc, plan, 32, st, nullptr, nullptr,
-                                      ceil_div(n, int64_t(32) * kVmax));
+      reinterpret_cast<uintptr_t>(C) % 16 == 0) {
+    const int w = spmm_team_tile_bytes(n * int64_t(sizeof(S)), n_cols, plan.tile_bytes);
+    const int T = w / 16;
+    return spmm_launch_team<DT, COMP>(data, idx, ptr, B, ldb, n, C, ldc, plan, T, ceil_div(n, int64_t(T) * kVmax),
+                                      st);
+  }
   const int v = spmm_pick_v<DT>(B, ldb, C, ldc, n);
   if constexpr (kVmax >= 8)
     if (v == 8) return spmm_launch_v<DT, 8, COMP>(data, idx, ptr, B, ldb, n, C, ldc, plan, st);
@@ -1015,9 +1326,10 @@ int spmm_dispatch(const void* data, const int32_t* idx, const int64_t* ptr, cons
 
 template <int DT>
 int spmm_mode(const void* data, const int32_t* idx, const int64_t* ptr, const void* B, int64_t ldb, int64_t n,
-              void* C, int64_t ldc, const fsb_spmv_plan& plan, cudaStream_t st) {
-  if (plan.flags & FSB_SPMM_COMPENSATED) return spmm_dispatch<DT, true>(data, idx, ptr, B, ldb, n, C, ldc, plan, st);
-  return spmm_dispatch<DT, false>(data, idx, ptr, B, ldb, n, C, ldc, plan, st);
+              int64_t n_cols, void* C, int64_t ldc, const fsb_spmv_plan& plan, cudaStream_t st) {
+  if (plan.flags & FSB_SPMM_COMPENSATED)
+    return spmm_dispatch<DT, true>(data, idx, ptr, B, ldb, n, n_cols, C, ldc, plan, st);
+  return spmm_dispatch<DT, false>(data, idx, ptr, B, ldb, n, n_cols, C, ldc, plan, st);
 }
 
 }  // namespace
@@ -1037,7 +1349,7 @@ int fsb_spmm_scratch_layout(int dtype, int64_t n, int64_t* partial_bytes_per_slo
   if (n < 0 || !partial_bytes_per_slot || !tickets_per_slot) return FSB_ERR_INVALID_ARG;
   const int64_t comps = (dtype == FSB_C64 || dtype == FSB_C128) ? 2 : 1;
   *partial_bytes_per_slot = spmm_pstride(n) * comps * 2 * rb;
-  *tickets_per_slot = spmm_cps(n);
+  *tickets_per_slot = spmm_cps_bytes(n, spmm_elem_bytes(dtype));
   return FSB_OK;
 }
 
@@ -1054,12 +1366,12 @@ int fsb_spmm_csr(int dtype, const void* data, const int32_t* indices, const int6
   if (plan->n_units >= INT32_MAX) return FSB_ERR_UNSUPPORTED;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   switch (dtype) {
-    case FSB_F16: return spmm_mode<FSB_F16>(data, indices, indptr, B, ldb, n, C, ldc, *plan, st);
-    case FSB_BF16: return spmm_mode<FSB_BF16>(data, indices, indptr, B, ldb, n, C, ldc, *plan, st);
-    case FSB_F32: return spmm_mode<FSB_F32>(data, indices, indptr, B, ldb, n, C, ldc, *plan, st);
-    case FSB_F64: return spmm_mode<FSB_F64>(data, indices, indptr, B, ldb, n, C, ldc, *plan, st);
-    case FSB_C64: return spmm_mode<FSB_C64>(data, indices, indptr, B, ldb, n, C, ldc, *plan, st);
-    case FSB_C128: return spmm_mode<FSB_C128>(data, indices, indptr, B, ldb, n, C, ldc, *plan, st);
+    case FSB_F16: return spmm_mode<FSB_F16>(data, indices, indptr, B, ldb, n, n_cols, C, ldc, *plan, st);
+    case FSB_BF16: return spmm_mode<FSB_BF16>(data, indices, indptr, B, ldb, n, n_cols, C, ldc, *plan, st);
+    case FSB_F32: return spmm_mode<FSB_F32>(data, indices, indptr, B, ldb, n, n_cols, C, ldc, *plan, st);
+    case FSB_F64: return spmm_mode<FSB_F64>(data, indices, indptr, B, ldb, n, n_cols, C, ldc, *plan, st);
+    case FSB_C64: return spmm_mode<FSB_C64>(data, indices, indptr, B, ldb, n, n_cols, C, ldc, *plan, st);
+    case FSB_C128: return spmm_mode<FSB_C128>(data, indices, indptr, B, ldb, n, n_cols, C, ldc, *plan, st);
     default: return FSB_ERR_UNSUPPORTED;
   }
 }

@@ -28,8 +28,9 @@
 // (sparse_operations/spmv_csr.py:179-240) and the bucketed CSR-vector kernels
 // (spmv_csr.py:247-368) of flagos-ai/FlagSparse.
 #include <algorithm>
-#include <atomic>
 #include <mutex>
+
+#include <cuda.h>
 #include <type_traits>
 
 #include "fsb_common.cuh"
@@ -556,30 +557,75 @@ constexpr int64_t kStaticTicketOffset = kStaticSlots * kStaticPartialBytes;
 static __device__ __align__(256) unsigned char g_spmv_static_scratch[kStaticTicketOffset + kStaticSlots * sizeof(int32_t)];
 
 constexpr int kStaticMaxDevices = 256;
-static std::atomic<void*> g_static_addr[kStaticMaxDevices];
+struct StaticScratchEntry {
+  unsigned long long ctx_id;  // the context the address was resolved in (0: none yet)
+  void* addr;
+};
+static StaticScratchEntry g_static_cache[kStaticMaxDevices];
 static std::mutex g_static_mu;
 
-// Device address of the current device's scratch; resolved once per device.
-static int static_scratch_address(void** out) {
+// Unique id of the calling thread's current context, 0 if there is none or the
+// driver cannot tell.  A device reset (or a new primary context) gives a new
+// id, so an address resolved in an earlier context is never reused.
+typedef CUresult (*PfnCtxGetCurrent)(CUcontext*);
+typedef CUresult (*PfnCtxGetId)(CUcontext, unsigned long long*);
+static unsigned long long current_context_id() {
+  static PfnCtxGetCurrent get_current = nullptr;
+  static PfnCtxGetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<PfnCtxGetCurrent>(p);
+    else
+      (void)cudaGetLastError();
+    p = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<PfnCtxGetId>(p);
+    else
+      (void)cudaGetLastError();
+  });
+  if (!get_current || !get_id) return 0;
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+  if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// Device address of the current device's scratch.  cudaGetSymbolAddress runs
+// once per device and context: on the first call, and again only after the
+// device's context changed (a device reset).  `st` must belong to the current
+// device: the scratch of another device is not reachable through it.
+static int static_scratch_address(cudaStream_t st, void** out) {
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess) {
     (void)cudaGetLastError();
     return FSB_ERR_CUDA;
   }
   if (dev < 0 || dev >= kStaticMaxDevices) return FSB_ERR_UNSUPPORTED;
-  void* p = g_static_addr[dev].load(std::memory_order_acquire);
-  if (!p) {
-    std::lock_guard<std::mutex> lock(g_static_mu);
-    p = g_static_addr[dev].load(std::memory_order_relaxed);
-    if (!p) {
-      if (cudaGetSymbolAddress(&p, g_spmv_static_scratch) != cudaSuccess || !p) {
-        (void)cudaGetLastError();
-        return FSB_ERR_CUDA;
-      }
-      g_static_addr[dev].store(p, std::memory_order_release);
-    }
+  int sdev = -1;
+  if (cudaStreamGetDevice(st, &sdev) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return FSB_ERR_INVALID_ARG;
   }
-  *out = p;
+  if (sdev != dev) return FSB_ERR_INVALID_ARG;
+  const unsigned long long ctx = current_context_id();
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  StaticScratchEntry& e = g_static_cache[dev];
+  if (!e.addr || (ctx != 0 && e.ctx_id != ctx)) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_spmv_static_scratch) != cudaSuccess || !p) {
+      (void)cudaGetLastError();
+      return FSB_ERR_CUDA;
+    }
+    e.addr = p;
+    e.ctx_id = current_context_id();  // the symbol lookup made the device's context current
+  }
+  *out = e.addr;
   return FSB_OK;
 }
 
@@ -632,7 +678,7 @@ int fsb_spmv_csr_static_scratch(int dtype, const void* data, const void* indices
   p.counters = nullptr;
   if (p.n_slots > 0) {
     void* base = nullptr;
-    const int rc = static_scratch_address(&base);
+    const int rc = static_scratch_address(static_cast<cudaStream_t>(stream), &base);
     if (rc != FSB_OK) return rc;
     p.partials = base;
     p.counters = reinterpret_cast<int32_t*>(static_cast<unsigned char*>(base) + kStaticTicketOffset);

@@ -256,8 +256,10 @@ class SpmmPlan:
     def n_slots(self):
         return self.plan.n_slots
 
-    def struct_for(self, n, compensated=False):
-        """ctypes reference to an fsb_spmv_plan with scratch for dense width ``n``."""
+    def struct_for(self, n, compensated=False, tile_bytes=0):
+        """ctypes reference to an fsb_spmv_plan with scratch for dense width ``n``.
+
+        ``tile_bytes``: column tile of the team kernel (0 = the library's choice)."""
         key = int(n)
         entry = self._scratch.get(key)
         if entry is None:
@@ -275,6 +277,7 @@ class SpmmPlan:
             self._scratch[key] = entry
         st = entry[2]
         st.flags = nat.FSB_SPMM_COMPENSATED if compensated else 0
+        st.tile_bytes = int(tile_bytes)
         return ctypes.byref(st)
 
     def counters_clear(self):
@@ -326,18 +329,19 @@ def spmm_backward(vals, perm32, t_indices, t_indptr, n_rows, n_cols, dY, X, dX, 
     return True
 
 
-def spmm(data, indices, indptr, n_rows, n_cols, B, plan, out, compensated=False):
+def spmm(data, indices, indptr, n_rows, n_cols, B, plan, out, compensated=False, tile_bytes=0):
     """out[:n_rows, :N] = A @ B through fsb_spmm_csr.
 
     ``indices`` int32, ``indptr`` int64, ``B`` and ``out`` row-major 2-D with
-    unit column stride; ``plan`` a SpmmPlan of this matrix.
+    unit column stride; ``plan`` a SpmmPlan of this matrix; ``tile_bytes`` the
+    column tile of the team kernel (0 = the library's choice).
     """
     n = int(B.shape[1])
     nat.check(
         nat.lib().fsb_spmm_csr(
             nat.dtype_code(data.dtype), nat.ptr(data), nat.ptr(indices), nat.ptr(indptr), int(n_rows), int(n_cols),
             nat.ptr(B), int(B.stride(0)) if B.shape[0] > 1 else max(n, 1), n, nat.ptr(out),
-            int(out.stride(0)) if out.shape[0] > 1 else max(n, 1), plan.struct_for(n, compensated),
+            int(out.stride(0)) if out.shape[0] > 1 else max(n, 1), plan.struct_for(n, compensated, tile_bytes),
             nat.stream_of(out.device),
         ),
         "fsb_spmm_csr",

@@ -21,6 +21,11 @@ class PreparedBsr16:
 
     __slots__ = ("blocks", "packed", "indices", "indptr", "shape", "n_brows", "n_bcols", "nnzb", "_err")
 
+    # _err: one int32 in pinned host memory, which the kernel writes (a plain
+    # store through the mapped address) when a bounded wait inside it expires.
+    # The host reads it without synchronising: every call checks the word left
+    # by earlier calls before it launches, and status() reports it on demand.
+
     def __init__(self, blocks, indices, indptr, shape):
         self.blocks = blocks
         # the blocks in the tensor cores' shared-memory layout, built once
@@ -33,7 +38,21 @@ class PreparedBsr16:
         self.n_brows = self.shape[0] // 16
         self.n_bcols = self.shape[1] // 16
         self.nnzb = int(indices.numel())
-        self._err = torch.zeros(1, dtype=torch.int32, device=blocks.device)
+        self._err = torch.zeros(1, dtype=torch.int32).pin_memory()
+
+    def status(self, synchronize=False):
+        """0, or 1 once a launch on this matrix gave up a bounded wait (its C is invalid).
+
+        ``synchronize`` first waits for the work queued on the current stream."""
+        if synchronize:
+            torch.cuda.current_stream(self.blocks.device).synchronize()
+        return int(self._err[0])
+
+    def _raise_if_failed(self, when):
+        if int(self._err[0]) != 0:
+            self._err.zero_()
+            raise RuntimeError(f"fsb_bsr16_spmm: a bounded wait inside the kernel expired ({when}); "
+                               "the output of that call is invalid")
 
 
 def prepare_spmm_bsr16(blocks, indices, indptr, shape):
@@ -77,8 +96,10 @@ def flagsparse_spmm_bsr16(blocks=None, indices=None, indptr=None, B=None, shape=
                           check_status=False):
     """C = A @ B for a BSR-16 matrix A on the tensor cores; returns C [M, N] in A's dtype.
 
-    ``check_status`` reads the kernel's error word back (one synchronisation)
-    and raises if a bounded wait inside the kernel gave up.
+    A failed launch (a bounded wait inside the kernel gave up) is reported
+    without a synchronisation by the next call on the same prepared matrix,
+    which raises before launching.  ``check_status`` waits for this call's
+    kernel instead (one stream synchronisation) and raises at once.
     """
     if prepared is None:
         if any(v is None for v in (blocks, indices, indptr, shape)):
@@ -97,6 +118,7 @@ def flagsparse_spmm_bsr16(blocks=None, indices=None, indptr=None, B=None, shape=
     n = int(B.shape[1])
     if n % 64:
         raise ValueError("B.shape[1] must be a multiple of 64 for the tensor-core BSR path")
+    prepared._raise_if_failed("an earlier call")
     B = B.contiguous()
     M = prepared.shape[0]
     if out is not None:
@@ -113,7 +135,7 @@ def flagsparse_spmm_bsr16(blocks=None, indices=None, indptr=None, B=None, shape=
         ),
         "fsb_bsr16_spmm",
     )
-    if check_status and int(prepared._err.item()) != 0:
-        prepared._err.zero_()
-        raise RuntimeError("fsb_bsr16_spmm: a bounded wait inside the kernel expired")
+    if check_status:
+        torch.cuda.current_stream(B.device).synchronize()
+        prepared._raise_if_failed("this call")
     return C

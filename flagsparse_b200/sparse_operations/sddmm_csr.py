@@ -5,10 +5,11 @@ Drop-in mirror of FlagSparse ``sparse_operations/sddmm_csr.py``: the same
 pattern validation messages (``:60-92``), ``prepare_sddmm_csr`` (``:107-118``),
 dense-input checks (``:219-243``), output checks (``:246-257``), diagnostic
 variants (``:260-288``), ``_run_sddmm_prepared`` meta (``:291-384``),
-``flagsparse_sddmm_csr`` (``:387-468``) and ``_sddmm_reference``
-(``:471-483``).  The compute is ``fsb_sddmm_csr``; ``allow_fallback`` is
-accepted for signature compatibility but there is no fallback path: a native
-failure raises.
+and ``flagsparse_sddmm_csr`` (``:387-468``).  The compute is
+``fsb_sddmm_csr``; ``allow_fallback`` is accepted for signature
+compatibility but there is no fallback path (FlagSparse's torch fallback,
+``_sddmm_reference`` at ``:471-483``, is not provided): a native failure
+raises.
 """
 
 import time
@@ -269,15 +270,3 @@ def flagsparse_sddmm_csr(data=None, indices=None, indptr=None, x=None, y=None, s
         return out_tensor, {"prepare_ms": prepare_ms, **launch_meta}
     return out_tensor
 
-
-def _sddmm_reference(indices, indptr, x, y, data, alpha, beta):
-    """The reference's torch formulation (sddmm_csr.py:471-483), used by tests as a cross-check."""
-    n_rows = int(indptr.numel()) - 1
-    row_ids = torch.repeat_interleave(torch.arange(n_rows, dtype=torch.int64, device=indices.device),
-                                      indptr[1:] - indptr[:-1])
-    if row_ids.numel() == 0:
-        return torch.empty(0, dtype=x.dtype, device=x.device)
-    vals = alpha * torch.sum(x[row_ids] * y[indices.to(torch.int64)], dim=1)
-    if data is not None:
-        vals = vals + beta * data
-    return vals

@@ -189,8 +189,9 @@ typedef struct fsb_spmv_plan {
   void* partials;            /* scratch: n_slots * fsb_spmv_partial_bytes(dtype) bytes       */
   int32_t* counters;         /* scratch: n_slots int32, zero before the first call; every
                                 call leaves them zero again                                  */
-  int32_t flags;             /* FSB_SPMV_* bits                                              */
-  int32_t reserved;
+  int32_t flags;             /* FSB_SPMV_* / FSB_SPMM_* bits                                 */
+  int32_t tile_bytes;        /* SpMM only: column tile of the team kernel in bytes (rounded
+                                up to a power of two, 16 .. 512); 0 = the library's choice    */
 } fsb_spmv_plan;
 
 /* Sum the rows of row-block units (rows of <= cap nonzeros) with plain
@@ -239,11 +240,14 @@ FSB_API int fsb_spmv_csr(int dtype, const void* data, const void* indices, int i
  * default chunk).
  *
  * The scratch is the current device's: `stream` must belong to the device
- * current on the calling thread.  The first call on a device resolves the
- * scratch address with cudaGetSymbolAddress (once per device, device current,
- * status checked; failure returns FSB_ERR_CUDA); make that first call before
- * any stream capture begins.  Every call clears the n_slots tickets the plan
- * uses (cudaMemsetAsync on `stream`) before its kernel.
+ * current on the calling thread (checked with cudaStreamGetDevice; a stream
+ * of another device gives FSB_ERR_INVALID_ARG).  The first call on a device
+ * resolves the scratch address with cudaGetSymbolAddress (once per device,
+ * device current, status checked; failure returns FSB_ERR_CUDA); make that
+ * first call before any stream capture begins.  The address is kept per
+ * device and context: after a device reset the next call resolves it again
+ * (and is then again a first call).  Every call clears the n_slots tickets
+ * the plan uses (cudaMemsetAsync on `stream`) before its kernel.
  *
  * One scratch per device: calls whose kernels can overlap on the GPU (other
  * streams, other threads, other plans) race on it and give wrong results.
@@ -355,8 +359,11 @@ FSB_API int fsb_sddmm_csr(int dtype, const int32_t* row_ids, const int32_t* indi
  * TMA; C: (16 n_brows) x n, row stride ldc, written in the value type (block
  * rows without blocks give zero rows).  n must be a multiple of 64 (a
  * 128-column tile whose upper half lies past n loads and stores only its
- * lower half) and ldb of 8.  d_error (device int) is set to 1 if a bounded
- * wait inside the kernel expired.
+ * lower half) and ldb of 8.  d_error is set to 1 if a bounded wait inside
+ * the kernel expired (the kernel then stops, lets its copies and MMAs finish
+ * and frees its tensor memory; C is not valid).  It is written with a plain
+ * store and never cleared, so it may be device memory or mapped pinned host
+ * memory that the host polls without synchronising.
  * No FlagSparse counterpart: its BSR support is SpMV (spmv_bsr.py).
  * ------------------------------------------------------------------------ */
 FSB_API int fsb_bsr16_pack(int dtype, const void* blocks, int64_t nnzb, void* packed, void* stream);

@@ -1,4 +1,5 @@
-"""Generate golden vectors by running FlagSparse's own code on small seeded inputs.
+"""Generate golden vectors by running FlagSparse's own code on seeded inputs: small
+cases whole, and sampled rows of the full-size configurations 2-4.
 
 Runs only where the FlagSparse source tree is available (pass its ``src``
 directory as argv[1]); the committed ``*.npz`` files are what the tests read.
@@ -275,6 +276,82 @@ def mtx_cases(tests_dir, out):
         out[f"mtx_{tag}_shape"] = np.array(shape, dtype=np.int64)
 
 
+def sample_rows(indptr, n_long, n_random, seed):
+    """The n_long longest rows plus n_random other rows (sorted, distinct)."""
+    lens = np.diff(indptr)
+    longest = np.argsort(-lens, kind="stable")[:n_long]
+    rest = np.setdiff1d(np.arange(lens.size), longest)
+    rnd = np.random.Generator(np.random.PCG64(seed)).choice(rest, n_random, replace=False)
+    return np.sort(np.concatenate([longest, rnd]))
+
+
+def sub_csr(c, rows):
+    """Rows `rows` of CSR c with all of its columns: (indptr, indices, positions taken)."""
+    lens = np.diff(c["indptr"])[rows]
+    ptr = np.zeros(rows.size + 1, dtype=np.int64)
+    np.cumsum(lens, out=ptr[1:])
+    take = np.concatenate([np.arange(c["indptr"][r], c["indptr"][r + 1]) for r in rows])
+    return ptr, c["indices"][take], take
+
+
+def config_cases(m, sm, dm, out):
+    """FlagSparse's own kernels on sampled rows of the full-size configurations.
+
+    Each of its kernels computes a row (SpMV, SpMM) or a nonzero (SDDMM) from
+    that row's entries and the dense operands alone, so its output on a
+    row subset equals those rows of its output on the whole matrix.  The tests
+    regenerate the same seeded inputs and compare the native result on the
+    whole matrix at these rows.
+    """
+    # configuration 2: 2,000,000 x 2,000,000 Zipf(2), fp32 and the fp64 drop-in
+    c = workloads.zipf_csr()
+    rows = sample_rows(c["indptr"], 6, 250, seed=41)
+    ptr, idx, take = sub_csr(c, rows)
+    out["config2_rows"] = rows
+    for dname in ("float32", "float64"):
+        dt = TORCH_DT[dname]
+        data = torch.from_numpy(c["data"][take]).to(dt)
+        x = torch.from_numpy(c["x"]).to(dt)
+        p = ref_prepared_spmv(m, data, torch.from_numpy(idx), torch.from_numpy(ptr), (rows.size, c["shape"][1]),
+                              "non")
+        out[f"config2_{dname}_y"] = np_of(m._triton_spmv_csr_impl_prepared(p, x))
+        buckets = m._build_spmv_opt_buckets(p.row_lengths, p.max_row_nnz, torch.int32, fp64=dt == torch.float64)
+        out[f"config2_{dname}_yopt"] = np_of(m._triton_spmv_csr_impl_opt_prepared(p, x, opt_buckets=buckets))
+    del c
+    # configuration 3: 1,000,000 x 1,000,000 power law (mean ~30), fp32, B = dense_normal(K, 64, seed 2)
+    c = workloads.zipf_csr(n=1_000_000, scale=32.0 / workloads.ZIPF_MEAN_UNSCALED, seed=2, dtype=np.float32,
+                           values="normal")
+    rows = sample_rows(c["indptr"], 4, 150, seed=42)
+    ptr, idx, take = sub_csr(c, rows)
+    B = torch.from_numpy(workloads.dense_normal(c["shape"][1], 64, seed=2))
+    indptr_t = torch.from_numpy(ptr)
+    max_row = int(np.diff(ptr).max())
+    launch = sm._resolve_spmm_base_triton_launch(torch.float32, 64, max_row)
+    C = sm._triton_spmm_csr_impl(
+        torch.from_numpy(c["data"][take]), torch.from_numpy(idx).to(torch.int32), indptr_t, B, rows.size, 64,
+        block_n=launch["block_n"], block_nnz=launch["block_nnz"], num_warps=launch["num_warps"],
+        num_stages=launch["num_stages"],
+    )
+    out["config3_rows"] = rows
+    out["config3_float32_N64_C"] = np_of(C)
+    del c, B
+    # configuration 4: SDDMM of dY and X (500,000 x 128 each, dense_normal seeds 3 and 4) on the
+    # Chung-Lu graph's pattern, fp32 (out[p] = <dY[row(p)], X[col(p)]>)
+    g = workloads.chung_lu_graph()
+    rows = sample_rows(g["indptr"], 4, 150, seed=43)
+    ptr, idx, take = sub_csr(g, rows)
+    dY = torch.from_numpy(workloads.dense_normal(g["shape"][0], 128, seed=3))[torch.from_numpy(rows)]
+    X = torch.from_numpy(workloads.dense_normal(g["shape"][1], 128, seed=4))
+    indptr_t = torch.from_numpy(ptr)
+    row_ids = dm._build_row_ids(indptr_t)
+    bk, nw = dm._resolve_sddmm_launch_config(128)
+    prep = dm.SDDMMPrepared(indices=torch.from_numpy(idx).to(torch.int32), indptr=indptr_t,
+                            shape=(rows.size, g["shape"][1]), row_ids=row_ids, block_k=bk, num_warps=nw)
+    res, _meta = dm._run_sddmm_prepared(prep, dY, X, None, 1.0, 0.0, None)
+    out["config4_rows"] = rows
+    out["config4_float32_K128_sddmm"] = np_of(res)
+
+
 def main():
     src = sys.argv[1] if len(sys.argv) > 1 else None
     if not src or not os.path.isdir(src):
@@ -294,6 +371,7 @@ def main():
         "golden_coo.npz": lambda o: coo_cases(m, o),
         "golden_bsr.npz": lambda o: bsr_cases(bm, o),
         "golden_mtx.npz": lambda o: mtx_cases(os.path.join(os.path.dirname(src), "tests"), o),
+        "golden_configs.npz": lambda o: config_cases(m, sm, dm, o),
     }
     only = set(sys.argv[2:])
     for fname, fn in groups.items():

@@ -1,4 +1,5 @@
-"""Differentiable CSR SpMM: gradients against finite differences and the oracle."""
+"""Differentiable CSR SpMM: gradients against finite differences, the oracle and torch's
+sparse autograd."""
 
 import numpy as np
 import pytest
@@ -81,6 +82,35 @@ def test_forward_backward_against_oracle(dname, thresh):
     assert _rel(host(Y).astype(np.float64), Yo) <= thresh
     assert _rel(host(X.grad).astype(np.float64), dXo) <= thresh
     assert _rel(host(vals.grad).astype(np.float64), dvo) <= thresh
+
+
+@pytest.mark.parametrize("dname,thresh", [("float64", 1e-12), ("float32", 1e-6), ("bfloat16", 1e-2),
+                                          ("float16", 5e-3)])
+def test_gradients_match_torch_sparse_autograd(dname, thresh):
+    """Y, dX and dvals against torch's own sparse autograd: torch.sparse.mm on a CPU
+    sparse_csr_tensor whose values are a leaf, float64, on the same rounded inputs
+    (20,000-node Chung-Lu graph, 64 features).  Half types are compared within
+    FlagSparse's thresholds; CPU sparse CSR matmul has no half kernels, so the
+    reference runs in float64 as the reference's own tests upcast."""
+    indptr, indices, data, shape = _graph(20_000, seed=4)
+    dt = getattr(torch, dname)
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    vals = dev(data, dt).requires_grad_(True)
+    X = torch.randn(shape[1], 64, device="cuda", generator=gen).to(dt).requires_grad_(True)
+    G = torch.randn(shape[0], 64, device="cuda", generator=gen).to(dt)
+    p = fs.prepare_spmm_csr_autograd(vals.detach(), dev(indices), dev(indptr), shape)
+    Y = fs.flagsparse_spmm_csr_autograd(vals, X, prepared=p)
+    Y.backward(G)
+
+    v64 = torch.from_numpy(host(vals).astype(np.float64)).requires_grad_(True)
+    X64 = torch.from_numpy(host(X).astype(np.float64)).requires_grad_(True)
+    A = torch.sparse_csr_tensor(torch.from_numpy(indptr), torch.from_numpy(indices.astype(np.int64)), v64,
+                                size=shape)
+    Yt = torch.sparse.mm(A, X64)
+    Yt.backward(torch.from_numpy(host(G).astype(np.float64)))
+    assert _rel(host(Y).astype(np.float64), Yt.detach().numpy()) <= thresh
+    assert _rel(host(X.grad).astype(np.float64), X64.grad.numpy()) <= thresh
+    assert _rel(host(vals.grad).astype(np.float64), v64.grad.numpy()) <= thresh
 
 
 def test_values_change_between_steps():
