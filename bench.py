@@ -347,6 +347,40 @@ class SpmvZipfSharded(SpmvZipf):
         return self.K * 4, self.rows * 4
 
 
+class SpmvGatherFloor(SpmvZipf):
+    """The x-gather floor of the headline SpMV (fsb_spmv_gather_floor): the fp64 sum of
+    data[i] * x[indices[i]] over all 38.9 M nonzeros of the 2M Zipf(2) matrix, with the
+    SpMV's own load kinds but no row structure.  value is reported on the SpMV's byte
+    model, so it reads as the SpMV's GB/s at that floor."""
+
+    name = "spmv_gather_floor_zipf2_2Mx2M_f32"
+
+    def __init__(self, device, seed=1):
+        super().__init__(device, seed)
+        from flagsparse_b200 import _native as nat
+
+        self.nat = nat
+        self.out = self.torch.empty(148 * 8, dtype=self.torch.float64, device=device)
+
+    def step(self):
+        nat = self.nat
+        nat.check(nat.lib().fsb_spmv_gather_floor(nat.dtype_code(self.data.dtype), nat.ptr(self.data),
+                                                  nat.ptr(self.indices), 0, self.nnz, nat.ptr(self.x),
+                                                  nat.ptr(self.out), self.out.numel(),
+                                                  nat.stream_of(self.data.device)),
+                  "fsb_spmv_gather_floor")
+
+    def e2e_step(self):
+        self.x_dev2.copy_(self.x_host, non_blocking=True)
+        self.step()
+
+    def e2e_bytes(self):
+        return self.K * 4, 0
+
+    def launches_per_step(self):
+        return 1
+
+
 class SpmvZipf64(SpmvZipf):
     """The headline matrix as the float64 drop-in: fp64 values, x and y (same pattern, seed 1)."""
 
@@ -806,6 +840,7 @@ class BatchedMix:
 
 
 CASES = {
+    "gather_floor": lambda d: SpmvGatherFloor(d),
     "batched_f32": lambda d: BatchedMix(d),
     "bsr16_bf16_N128": lambda d: Bsr16(d, 128),
     "bsr16_bf16_N64": lambda d: Bsr16(d, 64),
@@ -847,6 +882,7 @@ def measure_extras(torch, device, flush, peak):
     out["spmm_powerlaw_1Mx1M"] = dict(spmm, nnz=nnz, rows=M, mean_row=round(nnz / M, 2),
                                       bytes_models="gather: nnz*(s_v+4)+(M+1)*8+nnz*N*s+M*N*s; "
                                                    "compulsory: nnz*(s_v+4)+K*N*s+M*N*s")
+    out["spmm_powerlaw_1Mx1M"]["cpu_reference_f32_N128"] = cpu_torch_spmm()
     layer = {}
     rows = None
     for dname in ("f32", "bf16"):
@@ -863,6 +899,7 @@ def measure_extras(torch, device, flush, peak):
         nnz = case.nnz
         del case, sd
     layer["bf16_speedup_vs_f32"] = round(layer["f32"]["fwd_bwd_ms"] / layer["bf16"]["fwd_bwd_ms"], 3)
+    layer["cpu_reference_f32"] = cpu_torch_autograd()
     out["autograd_chung_lu_500k_K128"] = dict(layer, nnz=nnz, error_reference="float64 on the GPU, 500 sampled rows")
     case = BatchedMix(device)
     ms = _event_median_ms(torch, case.step, flush)
@@ -884,6 +921,14 @@ def measure_extras(torch, device, flush, peak):
                                    "tensor_frac_of_measured_bf16": round(case.flops() / ms / 1e9 / bf16_peak, 4),
                                    "nnzb": case.nnzb, "bound": "hbm (12 flop/byte, far below the tensor ridge)"}
     del case
+    case = SpmvGatherFloor(device)
+    ms = _event_median_ms(torch, case.step, flush)
+    out["spmv_gather_floor_zipf2M_f32"] = {
+        "ms": round(ms, 4), "spmv_model_gbs": round(case.alg_bytes() / ms / 1e6, 1),
+        "hbm_frac": round(case.alg_bytes() / ms / 1e6 / peak, 3),
+        "what": "sum of data[i]*x[indices[i]] over every nonzero of the headline matrix (no rows): the time "
+                "its values, columns and x gathers alone take"}
+    del case
     case = SpmvZipf64(device)
     ms = _event_median_ms(torch, case.step, flush)
     out["spmv_f64_zipf2M"] = {"ms": round(ms, 4), "gbs": round(case.alg_bytes() / ms / 1e6, 1),
@@ -896,6 +941,52 @@ def measure_extras(torch, device, flush, peak):
                                 "hbm_frac": round(case.alg_bytes() / ms / 1e6 / peak, 3), "nnzb": case.nnzb,
                                 "bytes_model": "nnzb*(256*4+4)+(n_brows+1)*8+2*M*4"}
     return out
+
+
+def cpu_torch_spmm(reps=2):
+    """C = A B on the host cores through torch.sparse.mm on a CPU sparse_csr_tensor (the
+    reference's CPU path) for the 1M power-law matrix and a 128-column fp32 B."""
+    import torch
+
+    from flagsparse_b200 import workloads
+
+    nthreads = os.cpu_count() or 1
+    torch.set_num_threads(nthreads)
+    c = workloads.zipf_csr(n=1_000_000, scale=32.0 / workloads.ZIPF_MEAN_UNSCALED, seed=2, dtype=np.float32,
+                           values="normal")
+    A = torch.sparse_csr_tensor(torch.from_numpy(c["indptr"]), torch.from_numpy(c["indices"]),
+                                torch.from_numpy(c["data"]), size=c["shape"])
+    B = torch.from_numpy(workloads.dense_normal(c["shape"][1], 128, seed=2))
+    s_per, n = _wall_per_step(lambda: torch.sparse.mm(A, B), 0.0, max_reps=reps)
+    return {"ms": round(s_per * 1e3, 2), "cores": nthreads, "kind": "reference",
+            "sample": f"{n} SpMMs through torch.sparse.mm on a CPU sparse_csr_tensor, fp32"}
+
+
+def cpu_torch_autograd(reps=2):
+    """Forward Y = A X and backward (dX, and dA on A's pattern) on the host cores through
+    torch's sparse CSR autograd (torch.sparse.mm with A a leaf) on the 500,000-node Chung-Lu
+    graph, fp32, K = 128."""
+    import torch
+
+    from flagsparse_b200 import workloads
+
+    nthreads = os.cpu_count() or 1
+    torch.set_num_threads(nthreads)
+    g = workloads.chung_lu_graph()
+    n = g["shape"][0]
+    X = torch.from_numpy(workloads.dense_normal(n, 128, seed=4)).requires_grad_(True)
+    dY = torch.from_numpy(workloads.dense_normal(n, 128, seed=3))
+    A = torch.sparse_csr_tensor(torch.from_numpy(g["indptr"]), torch.from_numpy(g["indices"].astype(np.int64)),
+                                torch.from_numpy(g["data"]), size=g["shape"], requires_grad=True)
+
+    def step():
+        A.grad = None
+        X.grad = None
+        torch.sparse.mm(A, X).backward(dY)
+
+    s_per, k = _wall_per_step(step, 0.0, max_reps=reps)
+    return {"fwd_bwd_ms": round(s_per * 1e3, 2), "cores": nthreads, "kind": "reference",
+            "sample": f"{k} forward + backward steps through torch's sparse CSR autograd on the host, fp32"}
 
 
 def _cpu_measure(make_workload_host, budget_s, nthreads):

@@ -185,7 +185,7 @@ template <typename S>
 __global__ void __launch_bounds__(kBsrThreads, kBsrCtasPerSm)
 k_bsr16_spmm(const __grid_constant__ CUtensorMap tmap_b, const S* __restrict__ packed, const int32_t* __restrict__ bcol,
              const int64_t* __restrict__ bptr, int64_t n_brows, int64_t rows_per_cta, S* __restrict__ C, int64_t ldc,
-             int64_t n, uint32_t idesc, int* __restrict__ err) {
+             int64_t n, uint32_t idesc, int tile_cols, int* __restrict__ err) {
   extern __shared__ unsigned char smem_raw[];
   const uint32_t raw = smem_addr(smem_raw);
   const uint32_t base = (raw + 1023u) & ~1023u;
@@ -199,13 +199,13 @@ k_bsr16_spmm(const __grid_constant__ CUtensorMap tmap_b, const S* __restrict__ p
   const int64_t r0 = int64_t(blockIdx.x) * rows_per_cta;
   const int64_t r1 = r0 + rows_per_cta < n_brows ? r0 + rows_per_cta : n_brows;
   if (r0 >= r1) return;  // the whole CTA, before any allocation
-  const int64_t col0 = int64_t(blockIdx.y) * kBsrTileM;
+  const int64_t col0 = int64_t(blockIdx.y) * tile_cols;
   const int64_t b0 = bptr[r0], total = bptr[r1] - b0;
 
-  // a tile's upper 64 columns may lie past N (N a multiple of 64): that half of
-  // the B slab is neither loaded nor stored
-  const bool upper = col0 + 64 < n;
-  if (warp < 4 && col0 + tid < n) {  // block rows without blocks get zero rows
+  // a tile's upper 64 columns may lie past N (N a multiple of 64), or the tile
+  // is 64 columns wide: that half of the B slab is neither loaded nor stored
+  const bool upper = tile_cols == kBsrTileM && col0 + 64 < n;
+  if (warp < 4 && tid < tile_cols && col0 + tid < n) {  // block rows without blocks get zero rows
     for (int64_t r = r0; r < r1; ++r) {
       if (bptr[r] == bptr[r + 1]) {
         S* c = C + r * 16 * ldc + col0 + tid;
@@ -322,7 +322,7 @@ k_bsr16_spmm(const __grid_constant__ CUtensorMap tmap_b, const S* __restrict__ p
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(acce0 + 8 * buf);
-      if (col0 + warp * 32 + lane < n) {
+      if (warp * 32 + lane < tile_cols && col0 + warp * 32 + lane < n) {
         S* c = C + r * 16 * ldc + col0 + warp * 32 + lane;
 #pragma unroll
         for (int q = 0; q < 16; ++q) store_out(c + q * ldc, __uint_as_float(v[q]));
@@ -379,14 +379,19 @@ int bsr_launch(CUtensorMapDataType tdt, uint32_t ab_format, const void* packed, 
              CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return FSB_ERR_UNSUPPORTED;
-  const int64_t tiles = ceil_div(n, kBsrTileM);
+  // 128-column tiles.  (64-column tiles when B exceeds L2, so that only half of
+  // B is gathered at a time, measured slower on 65,536^2 blocks with N = 128:
+  // 0.53 against 0.36 ms, the blocks being read once per tile.)
+  const int tile_cols = kBsrTileM;
+  const int64_t tiles = ceil_div(n, tile_cols);
+  if (tiles > 65535) return FSB_ERR_UNSUPPORTED;
   const int64_t target = 148 * kBsrCtasPerSm;  // resident CTAs
   const int64_t rows_per_cta = ceil_div(n_brows, target);
   const int64_t grid_x = ceil_div(n_brows, rows_per_cta);
   dim3 grid((unsigned)grid_x, (unsigned)tiles);
   k_bsr16_spmm<S><<<grid, kBsrThreads, kSmemBytes, st>>>(map, static_cast<const S*>(packed), bcol, bptr, n_brows,
                                                          rows_per_cta, static_cast<S*>(C), ldc, n,
-                                                         umma_idesc(ab_format), err);
+                                                         umma_idesc(ab_format), tile_cols, err);
   FSB_LAUNCH_CHECK();
   return FSB_OK;
 }
@@ -422,7 +427,7 @@ int fsb_bsr16_spmm(int dtype, const void* packed, const int32_t* bcol, const int
   if (n % 64 != 0 || ldb % 8 != 0 || reinterpret_cast<uintptr_t>(B) % 16 != 0 ||
       reinterpret_cast<uintptr_t>(packed) % 16 != 0 || n_bcols * 16 > INT32_MAX || n > INT32_MAX)
     return FSB_ERR_UNSUPPORTED;
-  if (ceil_div(n, kBsrTileM) > 65535) return FSB_ERR_UNSUPPORTED;
+  if (ceil_div(n, 64) > 65535) return FSB_ERR_UNSUPPORTED;
   if (n_bcols == 0) {  // every block row is empty: C = 0 (no tensor map over an empty B)
     return cudaMemset2DAsync(C, size_t(ldc) * 2, 0, size_t(n) * 2, size_t(n_brows) * 16,
                              static_cast<cudaStream_t>(stream)) == cudaSuccess

@@ -29,6 +29,7 @@
 // (sparse_operations/spmm_csr.py:3373-3466, 144-339) and the bucketed
 // alg1 / alg2 / opt kernels (spmm_csr.py:1091-2449, spmm_csr_opt_alg2.py) of
 // flagos-ai/FlagSparse.
+#include <atomic>
 #include <cstring>
 #include <type_traits>
 
@@ -72,6 +73,19 @@ __device__ __forceinline__ void load_slice(const S* p, int nv, S (&out)[V]) {
       }
     }
   }
+}
+
+// One whole 16-byte slice at B + row * ldb (row, ldb < 2^32: a single wide
+// 32 x 32-bit multiply), no partial-slice test: the team kernels point lanes
+// without columns at a valid slice and discard what they load.  (L2
+// evict-last hints on these gathers, with evict-first on A and C, measured no
+// better: fp32 N = 128 on a 1,000,000-row power-law matrix kept its 11 % L2
+// hit rate.)
+template <typename S, int V>
+__device__ __forceinline__ void load_row16(const S* __restrict__ B, uint32_t row, uint32_t ldb, S (&out)[V]) {
+  static_assert(int(sizeof(S)) * V == 16, "one 16-byte slice");
+  const uint4 r = __ldg(reinterpret_cast<const uint4*>(B + static_cast<uint64_t>(row) * ldb));
+  memcpy(out, &r, 16);
 }
 
 // Output slices are written once: STREAM makes them streaming (evict-first)
@@ -249,6 +263,63 @@ template <> __device__ __forceinline__ __half ld_once<__half>(const __half* p) {
 }
 template <> __device__ __forceinline__ __nv_bfloat16 ld_once<__nv_bfloat16>(const __nv_bfloat16* p) {
   return __ushort_as_bfloat16(__ldcs(reinterpret_cast<const unsigned short*>(p)));
+}
+
+// Asynchronous global -> shared copies of one 4-, 8- or 16-byte element
+// (cp.async): every copy of a staging pass is in flight at once, with no
+// registers held; cp_async_wait_all() then __syncwarp() before reading.
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* dst, const void* src) {
+  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(src), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Stages values and columns [s0, s0 + cnt) (cnt <= MAXN) into the warp's
+// shared slices by cp.async, every copy in flight at once; returns the
+// offset of value s0 in sh_a (the values start at sh_a + the offset).  2-byte
+// values move as 4-byte words from the even element at or below s0 (offset 1
+// when s0 is odd; the slice holds MAXN + 2 values); a last value left alone
+// in its word is copied by itself, so nothing past value s0 + cnt - 1 is
+// read.  The caller's __syncwarp() makes the slices visible to all lanes.
+template <typename S, int MAXN>
+__device__ __forceinline__ int stage_nz(S* sh_a, int32_t* sh_c, const S* __restrict__ data,
+                                        const int32_t* __restrict__ col, int64_t s0, int cnt, int lane) {
+  int shift = 0;
+  for (int k = lane; k < cnt; k += 32) cp_async<4>(sh_c + k, col + s0 + k);
+  if constexpr (sizeof(S) >= 4) {
+    for (int k = lane; k < cnt; k += 32) cp_async<int(sizeof(S))>(sh_a + k, data + s0 + k);
+  } else {
+    shift = static_cast<int>(s0 & 1);
+    const S* base = data + (s0 - shift);  // 4-byte aligned (data is)
+    const int words = (cnt + shift) >> 1;
+    for (int w = lane; w < words; w += 32) cp_async<4>(sh_a + 2 * w, base + 2 * w);
+    if (((cnt + shift) & 1) && lane == 0) sh_a[cnt + shift - 1] = ld_once(data + s0 + cnt - 1);
+  }
+  cp_async_wait_all();
+  return shift;
+}
+
+// Run-local row offsets off[i] = ptr[r0 + i] - s0 for i <= nr (nr < MAXR),
+// every load issued before the first store.
+template <int MAXR>
+__device__ __forceinline__ void stage_offsets(int32_t* sh_off, const int64_t* __restrict__ ptr, int64_t r0, int nr,
+                                              int64_t s0, int lane) {
+  constexpr int kQ = (MAXR + 32) / 32;
+  int64_t v[kQ];
+#pragma unroll
+  for (int q = 0; q < kQ; ++q) {
+    const int i = lane + 32 * q;
+    if (i <= nr) v[q] = __ldg(ptr + r0 + i);
+  }
+#pragma unroll
+  for (int q = 0; q < kQ; ++q) {
+    const int i = lane + 32 * q;
+    if (i <= nr) sh_off[i] = static_cast<int32_t>(v[q] - s0);
+  }
 }
 
 // Rows of more than this many nonzeros accumulate with Dot2 in the types whose
@@ -442,14 +513,17 @@ k_spmm_csr(const typename VT<DT>::Store* __restrict__ data, const int32_t* __res
 constexpr int kRowUnits = 4;                            // row-block units per row group
 constexpr int kRowStage = kRowUnits * 2 * kSpmmMaxCap;  // staged nonzeros of a run (< 512)
 constexpr int kRowRows = kRowUnits * kSpmmMaxCap;       // rows of a run (<= 256)
-static_assert(kRowRows <= 256, "run-local row ids are 8-bit");
 static_assert(kSpmmBatch <= kRowStage, "the long-row batch must fit the run staging");
 
-// Per-warp slice: staged values, columns, run-local row ids (8-bit) and row
-// offsets, then (16-byte aligned) one parked accumulator per lane.
+// Per-warp slice: staged values, columns and run-local row offsets, then
+// (16-byte aligned) one parked accumulator per lane.
+template <typename S>
+constexpr int spmm_team_vals_bytes() {
+  return ((kRowStage + 2) * int(sizeof(S)) + 15) & ~15;  // 2-byte values may start one element early
+}
 template <typename S>
 constexpr int spmm_team_park_offset() {
-  return (kRowStage * (int(sizeof(S)) + 4 + 1) + (kRowRows + 1) * 4 + 15) & ~15;
+  return (spmm_team_vals_bytes<S>() + kRowStage * 4 + (kRowRows + 1) * 4 + 15) & ~15;
 }
 template <int DT, bool COMP>
 constexpr int spmm_team_warp_smem_bytes() {
@@ -458,17 +532,19 @@ constexpr int spmm_team_warp_smem_bytes() {
   return spmm_team_park_offset<S>() + 32 * int(sizeof(SpmmAcc<DT, COMP, V>));
 }
 
-// Resident blocks the register budget is sized for: 3 (85 registers), 2 for
-// complex fp64.
-template <int DT, bool COMP, bool FUSED>
+// Resident blocks the register budget is sized for: 4 (64 registers) for
+// plain sums of 2- and 4-byte values, 3 (85) for 8-byte values and for
+// compensated or fused sums, 2 for complex fp64.  More resident warps keep
+// more B rows in flight: wide rows measured up to 15 % faster at 4 blocks with
+// 4 slices ahead than at 3 blocks with 6 ahead.
+template <int DT, bool COMP, bool FUSED, int KP>
 struct SpmmTeamMinBlocks {
-  static constexpr int value = (DT == FSB_C128) ? 2 : 3;
+  static constexpr int value = (DT == FSB_C128) ? 2 : (!COMP && !FUSED && DT != FSB_F64 && DT != FSB_C64) ? 4 : 3;
 };
 
-// B-row slices a team loads ahead of its sums in the row walk
-template <int DT, bool COMP, bool FUSED>
-struct TeamSteps { static constexpr int value = (DT == FSB_F32 && !COMP && !FUSED) ? 8 : 4; };
-
+// B-row slices a team loads ahead of its sums in the row walk (KP): 4 for
+// teams narrower than the warp, 6 for 32-lane teams, whose warp walks its
+// rows alone and needs more of them in flight.
 template <int DT, bool COMP, int V>
 __device__ __forceinline__ void acc_shfl_add(SpmmAcc<DT, COMP, V>& a, int m) {
 #pragma unroll
@@ -508,15 +584,38 @@ __device__ __forceinline__ void acc_combine(SpmmAcc<DT, COMP, V>& a, const SpmmA
     }
 }
 
+// a += t elementwise, each add an error-free TwoSum into the compensated a
+template <int DT, int V>
+__device__ __forceinline__ void acc_fold(SpmmAcc<DT, true, V>& a, const SpmmAcc<DT, false, V>& t) {
+#pragma unroll
+  for (int c = 0; c < SpmmAcc<DT, true, V>::kNC; ++c)
+#pragma unroll
+    for (int j = 0; j < V; ++j) a.s[c][j].add(t.s[c][j].hi);
+}
+
+// Accumulation of a long-row chunk: MODE 0 plain sums; 1 Dot2 on every term
+// (plans with FSB_SPMM_COMPENSATED); 2 blocked compensation: each step's
+// kSpmmAhead products of a team are summed plainly, then folded into a Dot2
+// accumulator, so the error is at most gamma_(kSpmmAhead+1) * sum|a||b| plus
+// the final rounding whatever the row length (the chunk and team partials
+// are combined compensated as well).
+template <int DT, int MODE, int V>
+struct ChunkAcc;
+template <int DT, int V>
+struct ChunkAcc<DT, 0, V> { using T = SpmmAcc<DT, false, V>; };
+template <int DT, int V>
+struct ChunkAcc<DT, 1, V> { using T = SpmmAcc<DT, true, V>; };
+template <int DT, int V>
+struct ChunkAcc<DT, 2, V> { using T = SpmmAcc<DT, true, V>; };
+
 // One long-row chunk of the team kernel: team g takes nonzeros g, g+G, ...;
 // the team partials are combined by xor-shuffles over the team index, then
 // the chunk is stored directly (one-chunk rows) or as a slot partial whose
-// ticket's last taker adds the partials in chunk order.  ACOMP selects the
-// accumulator (Dot2 or plain).
-template <int DT, bool ACOMP, bool FUSED>
+// ticket's last taker adds the partials in chunk order.
+template <int DT, int MODE, bool FUSED>
 __device__ __forceinline__ void team_chunk(const typename VT<DT>::Store* __restrict__ data,
                                            const int32_t* __restrict__ col,
-                                           const typename VT<DT>::Store* __restrict__ B, int64_t ldb, int64_t n,
+                                           const typename VT<DT>::Store* __restrict__ B, uint32_t ldb, int64_t n,
                                            typename VT<DT>::Store* __restrict__ C, int64_t ldc,
                                            const fsb_spmv_plan& plan, const fsb_spmv_unit* ud, int T, int64_t tile,
                                            int64_t c0, int nv, int64_t pstride, int64_t cps,
@@ -526,24 +625,22 @@ __device__ __forceinline__ void team_chunk(const typename VT<DT>::Store* __restr
   using S = typename VT<DT>::Store;
   using R = typename VT<DT>::Real;
   constexpr int V = 16 / int(sizeof(S));
-  using Acc = SpmmAcc<DT, ACOMP, V>;
+  using Acc = typename ChunkAcc<DT, MODE, V>::T;
   constexpr int kER = Acc::kNC * 2;
   const int lane = threadIdx.x & 31;
   const int G = 32 / T, team = lane / T;
   const int64_t s0 = __ldg(&ud->nnz_begin), s1 = __ldg(&ud->nnz_end);
   const int32_t row = __ldg(&ud->row), tag = __ldg(&ud->tag);
   const int32_t nch = __ldg(&ud->n_chunks), slot = __ldg(&ud->slot);
+  const S* Bl = B + (nv > 0 ? c0 : 0);  // lanes without columns load column 0 and discard it
   Acc acc;
   acc.zero();
   YAcc<R> yacc;
   yacc.zero();
-  for (int64_t b0 = s0; b0 < s1; b0 += kSpmmBatch) {
-    const int cnt = static_cast<int>(s1 - b0 < kSpmmBatch ? s1 - b0 : int64_t(kSpmmBatch));
+  for (int64_t b0 = s0; b0 < s1; b0 += kRowStage) {
+    const int cnt = static_cast<int>(s1 - b0 < kRowStage ? s1 - b0 : int64_t(kRowStage));
     __syncwarp();
-    for (int k = lane; k < cnt; k += 32) {
-      sh_a[k] = ld_once(data + b0 + k);
-      sh_c[k] = ld_once(col + b0 + k);
-    }
+    const S* sv = sh_a + stage_nz<S, kRowStage>(sh_a, sh_c, data, col, b0, cnt, lane);
     __syncwarp();
     for (int k = 0; k < cnt; k += kSpmmAhead * G) {
       S bv[kSpmmAhead][V];
@@ -551,7 +648,7 @@ __device__ __forceinline__ void team_chunk(const typename VT<DT>::Store* __restr
 #pragma unroll
       for (int q = 0; q < kSpmmAhead; ++q) {
         const int kk = k + q * G + team;
-        load_slice<S, V>(B + int64_t(sh_c[kk < cnt ? kk : 0]) * ldb + c0, kk < cnt ? nv : 0, bv[q]);
+        load_row16<S, V>(Bl, static_cast<uint32_t>(sh_c[kk < cnt ? kk : cnt - 1]), ldb, bv[q]);
       }
       if constexpr (FUSED) {
         // the y terms of these kSpmmAhead * G items, one per lane in order
@@ -561,16 +658,27 @@ __device__ __forceinline__ void team_chunk(const typename VT<DT>::Store* __restr
           if (q * 32 + lane < kSpmmAhead * G && kk < cnt) xv[q] = ld_gather(x + sh_c[kk]);
         }
       }
+      if constexpr (MODE == 2) {
+        SpmmAcc<DT, false, V> step;
+        step.zero();
 #pragma unroll
-      for (int q = 0; q < kSpmmAhead; ++q) {
-        const int kk = k + q * G + team;
-        if (kk < cnt) acc.add(sh_a[kk], bv[q]);
+        for (int q = 0; q < kSpmmAhead; ++q) {
+          const int kk = k + q * G + team;
+          if (kk < cnt) step.add(sv[kk], bv[q]);
+        }
+        acc_fold(acc, step);
+      } else {
+#pragma unroll
+        for (int q = 0; q < kSpmmAhead; ++q) {
+          const int kk = k + q * G + team;
+          if (kk < cnt) acc.add(sv[kk], bv[q]);
+        }
       }
       if constexpr (FUSED) {
 #pragma unroll
         for (int q = 0; q * 32 < kSpmmAhead * G; ++q) {
           const int kk = k + q * 32 + lane;
-          if (q * 32 + lane < kSpmmAhead * G && kk < cnt) yacc.add_prod(to_real(sh_a[kk]), to_real(xv[q]));
+          if (q * 32 + lane < kSpmmAhead * G && kk < cnt) yacc.add_prod(to_real(sv[kk]), to_real(xv[q]));
         }
       }
     }
@@ -584,7 +692,7 @@ __device__ __forceinline__ void team_chunk(const typename VT<DT>::Store* __restr
     if (team == 0 && nv > 0) {
       S o[V];
       acc.result(o);
-      store_slice(C + int64_t(row) * ldc + c0, nv, o);
+      store_slice<S, V, true>(C + int64_t(row) * ldc + c0, nv, o);
     }
     if constexpr (FUSED)
       if (lane == 0 && tile == 0) put_y(y[row], yacc.value());
@@ -612,7 +720,7 @@ __device__ __forceinline__ void team_chunk(const typename VT<DT>::Store* __restr
     if (nv > 0) {
       S o[V];
       fin.result(o);
-      store_slice(C + int64_t(row) * ldc + c0, nv, o);
+      store_slice<S, V, true>(C + int64_t(row) * ldc + c0, nv, o);
     }
     if constexpr (FUSED) {
       if (lane == 0 && tile == 0) {
@@ -626,10 +734,10 @@ __device__ __forceinline__ void team_chunk(const typename VT<DT>::Store* __restr
   }
 }
 
-template <int DT, bool COMP, bool FUSED>
-__global__ void __launch_bounds__(kSpmmWarps * 32, SpmmTeamMinBlocks<DT, COMP, FUSED>::value)
+template <int DT, bool COMP, bool FUSED, int KP>
+__global__ void __launch_bounds__(kSpmmWarps * 32, SpmmTeamMinBlocks<DT, COMP, FUSED, KP>::value)
 k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __restrict__ col,
-            const int64_t* __restrict__ ptr, const typename VT<DT>::Store* __restrict__ B, int64_t ldb, int64_t n,
+            const int64_t* __restrict__ ptr, const typename VT<DT>::Store* __restrict__ B, uint32_t ldb, int64_t n,
             typename VT<DT>::Store* __restrict__ C, int64_t ldc, fsb_spmv_plan plan, int T, int64_t tiles,
             int64_t pstride, int64_t cps, const typename VT<DT>::Store* __restrict__ x,
             typename VT<DT>::Store* __restrict__ y) {
@@ -637,16 +745,18 @@ k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __re
   using R = typename VT<DT>::Real;
   constexpr int V = 16 / int(sizeof(S));
   using Acc = SpmmAcc<DT, COMP, V>;
-  constexpr int kP = TeamSteps<DT, COMP, FUSED>::value;
+  constexpr int kP = KP;
+  // the KP != 4 instantiation runs 32-lane teams only (one team per warp): a
+  // run's rows all end inside the team, so it has no scan and parks nothing
+  constexpr bool kOneTeam = KP != 4;
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int G = 32 / T, team = lane / T, tl = lane % T;
   unsigned char* wbase = smem_raw + warp * spmm_team_warp_smem_bytes<DT, COMP>();
   S* sh_a = reinterpret_cast<S*>(wbase);
-  int32_t* sh_c = reinterpret_cast<int32_t*>(wbase + kRowStage * sizeof(S));
+  int32_t* sh_c = reinterpret_cast<int32_t*>(wbase + spmm_team_vals_bytes<S>());
   int32_t* sh_off = sh_c + kRowStage;
-  uint8_t* sh_rid = reinterpret_cast<uint8_t*>(sh_off + kRowRows + 1);
   Acc* sh_park = reinterpret_cast<Acc*>(wbase + spmm_team_park_offset<S>()) + lane;
 
   const int64_t nb = plan.n_block_units;
@@ -659,6 +769,7 @@ k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __re
     const uint32_t tile = it / n_items, item = it - tile * n_items;
     const int64_t c0 = int64_t(tile) * (int64_t(T) * V) + int64_t(tl) * V;  // this lane's first column
     const int nv = c0 + V <= n ? V : 0;                       // n is a multiple of V
+    const S* Bl = B + (nv > 0 ? c0 : 0);  // lanes without columns load column 0 and discard it
     __syncwarp();  // the staging slice of the previous item is free
 
     if (item < n_groups) {
@@ -694,21 +805,13 @@ k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __re
         const int nr = r1 - r0;
         const int cnt = static_cast<int>(s1 - s0);
         __syncwarp();
-        for (int i = lane; i <= nr; i += 32) sh_off[i] = static_cast<int32_t>(__ldg(ptr + r0 + i) - s0);
-        for (int k = lane; k < cnt; k += 32) {
-          sh_a[k] = ld_once(data + s0 + k);
-          sh_c[k] = ld_once(col + s0 + k);
-        }
+        const S* sv = sh_a + stage_nz<S, kRowStage>(sh_a, sh_c, data, col, s0, cnt, lane);
+        stage_offsets<kRowRows>(sh_off, ptr, r0, nr, s0, lane);
         __syncwarp();
-        // run-local row of every nonzero; empty rows get zero slices (one team each)
+        // empty rows get zero slices (one team each)
         for (int i0 = 0; i0 < nr; i0 += 32) {
           const int i = i0 + lane;
-          bool empty = false;
-          if (i < nr) {
-            const int b = sh_off[i], e = sh_off[i + 1];
-            for (int k = b; k < e; ++k) sh_rid[k] = static_cast<uint8_t>(i);
-            empty = b == e;
-          }
+          const bool empty = i < nr && sh_off[i] == sh_off[i + 1];
           unsigned m = __ballot_sync(0xffffffffu, empty);
           for (int q = 0; m; ++q) {
             const int b = __ffs(m) - 1;
@@ -719,7 +822,7 @@ k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __re
                 z.zero();
                 S o[V];
                 z.result(o);
-                store_slice(C + (int64_t(r0) + i0 + b) * ldc + c0, nv, o);
+                store_slice<S, V, true>(C + (int64_t(r0) + i0 + b) * ldc + c0, nv, o);
               }
               if constexpr (FUSED)
                 if (tl == 0 && tile == 0) put_y(y[int64_t(r0) + i0 + b], 0.0f);
@@ -739,14 +842,23 @@ k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __re
         YAcc<R> yacc, ypark;
         yacc.zero();
         ypark.zero();
-        int cur = jb < je ? sh_rid[jb] : 0;
+        int cur = 0;  // the row of nonzero jb: the last row whose offset is <= jb
+        {
+          int lo = 0, hi = nr - 1;
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (sh_off[mid] <= jb) lo = mid; else hi = mid - 1;
+          }
+          cur = lo;
+        }
+        int next_end = jb < je ? sh_off[cur + 1] : 0;  // where row cur ends
         bool open_start = jb < je && sh_off[cur] < jb;  // row cur began in an earlier team
         int park_row = -1;
         auto put_row = [&](const Acc& a, const YAcc<R>& ya, int r) {
           if (nv > 0) {
             S o[V];
             a.result(o);
-            store_slice(C + (int64_t(r0) + r) * ldc + c0, nv, o);
+            store_slice<S, V, true>(C + (int64_t(r0) + r) * ldc + c0, nv, o);
           }
           if constexpr (FUSED)
             if (tl == 0 && tile == 0) put_y(y[int64_t(r0) + r], ya.value());
@@ -757,16 +869,15 @@ k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __re
 #pragma unroll
           for (int q = 0; q < kP; ++q) {  // past je: the last nonzero again, loaded and not summed
             const int j = j0 + q < je ? j0 + q : je - 1;
-            load_slice<S, V>(B + int64_t(sh_c[j]) * ldb + c0, nv, bv[q]);
+            load_row16<S, V>(Bl, static_cast<uint32_t>(sh_c[j]), ldb, bv[q]);
             if constexpr (FUSED) xv[q] = ld_gather(x + sh_c[j]);
           }
 #pragma unroll
           for (int q = 0; q < kP; ++q) {
             const int j = j0 + q;
             if (j < je) {
-              const int r = sh_rid[j];
-              if (r != cur) {  // row cur ended before nonzero j
-                if (open_start) {
+              if (j == next_end) {  // row cur ended before nonzero j
+                if (!kOneTeam && open_start) {
                   *sh_park = acc;  // finished after the scan
                   ypark = yacc;
                   park_row = cur;
@@ -776,15 +887,23 @@ k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __re
                 }
                 acc.zero();
                 yacc.zero();
-                cur = r;
+                do {  // past the empty rows (already zeroed) to the row of nonzero j
+                  ++cur;
+                  next_end = sh_off[cur + 1];
+                } while (next_end == j);
               }
-              const S a = sh_a[j];
+              const S a = sv[j];
               acc.add(a, bv[q]);
               if constexpr (FUSED) yacc.add_prod(to_real(a), to_real(xv[q]));
             }
           }
         }
-        const bool open_end = jb < je && sh_off[cur + 1] > je;  // row cur goes on in later teams
+        if constexpr (kOneTeam) {  // one team walked the whole run: its last row ends here
+          if (jb < je) put_row(acc, yacc, cur);
+          __syncwarp();
+          continue;
+        }
+        const bool open_end = jb < je && next_end > je;  // row cur goes on in later teams
         // inclusive segmented scan of the open-ended partials over the teams
         const int key = open_end ? cur : -1;
         Acc sc = acc;
@@ -832,12 +951,15 @@ k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __re
     const int32_t nch = __ldg(&ud->n_chunks);
     // rows of more than kCompensateAbove nonzeros sum with Dot2 (compensated)
     // accumulators in the fp32-accumulated types, partials and all
-    if (kCompLong<DT, COMP> && int64_t(nch) * plan.chunk_nnz > kCompensateAbove)
-      team_chunk<DT, COMP || kCompLong<DT, COMP>, FUSED>(data, col, B, ldb, n, C, ldc, plan, ud, T, tile, c0, nv,
-                                                         pstride, cps, x, y, sh_a, sh_c);
+    if constexpr (COMP)
+      team_chunk<DT, 1, FUSED>(data, col, B, ldb, n, C, ldc, plan, ud, T, tile, c0, nv, pstride, cps, x, y, sh_a,
+                               sh_c);
+    else if (kCompLong<DT, COMP> && int64_t(nch) * plan.chunk_nnz > kCompensateAbove)
+      team_chunk<DT, 2, FUSED>(data, col, B, ldb, n, C, ldc, plan, ud, T, tile, c0, nv, pstride, cps, x, y, sh_a,
+                               sh_c);
     else
-      team_chunk<DT, COMP, FUSED>(data, col, B, ldb, n, C, ldc, plan, ud, T, tile, c0, nv, pstride, cps, x, y, sh_a,
-                                  sh_c);
+      team_chunk<DT, 0, FUSED>(data, col, B, ldb, n, C, ldc, plan, ud, T, tile, c0, nv, pstride, cps, x, y, sh_a,
+                               sh_c);
   }
 }
 
@@ -974,19 +1096,38 @@ k_spmm_bwd(const typename VT<DT>::Store* __restrict__ vals, const int32_t* __res
   const int64_t s0 = __ldg(&ud->nnz_begin), s1 = __ldg(&ud->nnz_end);
   const int32_t row = __ldg(&ud->row), tag = __ldg(&ud->tag);
 
+  // stages a batch of <= kSpmmBatch nonzeros: every permutation and column
+  // load issued first, then every value gather, then the stores
   auto stage = [&](int64_t from, int cnt) {
-    for (int k = lane; k < cnt; k += 32) {
-      const int32_t p = ld_once(perm + from + k);
-      sh_p[k] = p;
-      sh_a[k] = vals[p];
-      sh_c[k] = ld_once(col + from + k);
+    constexpr int kQ = kSpmmBatch / 32;
+    int32_t pv[kQ], cv[kQ];
+    S av[kQ];
+#pragma unroll
+    for (int q = 0; q < kQ; ++q) {
+      const int k = lane + 32 * q;
+      if (k < cnt) {
+        pv[q] = ld_once(perm + from + k);
+        cv[q] = ld_once(col + from + k);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kQ; ++q)
+      if (lane + 32 * q < cnt) av[q] = vals[pv[q]];
+#pragma unroll
+    for (int q = 0; q < kQ; ++q) {
+      const int k = lane + 32 * q;
+      if (k < cnt) {
+        sh_p[k] = pv[q];
+        sh_a[k] = av[q];
+        sh_c[k] = cv[q];
+      }
     }
   };
   if (tag >= 0) {
     // ------------------------------------------------------------ row block
     const int nr = tag - row;
     const int cnt = static_cast<int>(s1 - s0);
-    for (int i = lane; i <= nr; i += 32) sh_off[i] = static_cast<int32_t>(__ldg(ptr + row + i) - s0);
+    stage_offsets<kSpmmMaxCap>(sh_off, ptr, row, nr, s0, lane);
     stage(s0, cnt);
     __syncwarp();
     for (int i0 = 0; i0 < nr; i0 += G) {
@@ -1138,12 +1279,14 @@ inline int64_t spmm_cps(int64_t n) { return spmm_cps_bytes(n, sizeof(typename VT
 
 // Column tile of the team kernel, in bytes (a power of two, 16 .. 512).  The
 // default is the whole row (rounded up to a power of two of 16-byte slices) up
-// to 512 bytes, halved down to 64 bytes while the tile's slice of B, n_cols x
-// tile bytes, exceeds kSpmmL2Slice: a slice that fits in L2 is gathered from
-// L2 after its first read, which pays for re-reading A once per tile.  A
-// positive `hint` (fsb_spmv_plan.tile_bytes) replaces the default.
-constexpr int64_t kSpmmL2Slice = int64_t(80) << 20;
-inline int spmm_team_tile_bytes(int64_t row_bytes, int64_t n_cols, int32_t hint) {
+// to 512 bytes.  A positive `hint` (fsb_spmv_plan.tile_bytes) asks for
+// narrower tiles: then only a tile's slice of B (n_cols x tile bytes) is
+// gathered at a time, which stays in L2 when it fits, at the cost of reading
+// A once per tile.  On B200 the whole-row tile measured faster for every
+// width up to 512 bytes on 1,000,000-row matrices (fp32 N = 128: 2.4 ms
+// against 3.6 ms at 128-byte and 5.5 ms at 64-byte tiles), so narrow tiles
+// are opt-in.
+inline int spmm_team_tile_bytes(int64_t row_bytes, int32_t hint) {
   int w = 16;
   while (w < row_bytes && w < 512) w *= 2;
   if (hint > 0) {
@@ -1151,30 +1294,7 @@ inline int spmm_team_tile_bytes(int64_t row_bytes, int64_t n_cols, int32_t hint)
     while (h < hint && h < 512) h *= 2;
     return h < w ? h : w;
   }
-  while (w > 64 && n_cols * w > kSpmmL2Slice) w /= 2;
   return w;
-}
-
-// Resident blocks per SM of a kernel at this block size and shared memory,
-// looked up once per kernel (and device ordinal) and kept.
-template <typename K>
-int64_t resident_blocks(K kern, int threads, size_t smem) {
-  static int cached[64] = {0};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
-    (void)cudaGetLastError();
-    return 148;
-  }
-  if (cached[dev] == 0) {
-    int per_sm = 0, sms = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || per_sm < 1 || sms < 1) {
-      (void)cudaGetLastError();
-      return 148;
-    }
-    cached[dev] = per_sm * sms;
-  }
-  return cached[dev];
 }
 
 template <int DT, int V, bool COMP>
@@ -1210,33 +1330,41 @@ int spmm_pick_v(const void* B, int64_t ldb, const void* C, int64_t ldc, int64_t 
   return v;
 }
 
-// The team kernel, persistent: at most the resident blocks, each warp striding
-// over the work items of every tile (tile bytes = T * 16).
+// The team kernel: one work item per warp, the items of every tile in tile
+// order (tile bytes = T * 16), so the blocks of one tile run together.
 template <int DT, bool COMP, bool FUSED = false>
 int spmm_launch_team(const void* data, const int32_t* idx, const int64_t* ptr, const void* B, int64_t ldb, int64_t n,
                      void* C, int64_t ldc, const fsb_spmv_plan& plan, int T, int64_t tiles, cudaStream_t st,
                      const void* x = nullptr, void* y = nullptr) {
   using S = typename VT<DT>::Store;
   const size_t smem = size_t(spmm_team_warp_smem_bytes<DT, COMP>()) * kSpmmWarps;
-  auto kern = k_spmm_team<DT, COMP, FUSED>;
-  static bool attr_set = false;  // per instantiation; the attribute is per function
-  if (!attr_set) {
-    if (smem > 48 * 1024 &&
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+  const int wide = (!FUSED && T == 32) ? 1 : 0;
+  auto kern = wide ? k_spmm_team<DT, COMP, FUSED, 6> : k_spmm_team<DT, COMP, FUSED, 4>;
+  if (smem > 48 * 1024) {  // opt in to the larger dynamic shared memory once per kernel and device
+    static std::atomic<uint64_t> done[2];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
       (void)cudaGetLastError();
       return FSB_ERR_CUDA;
     }
-    attr_set = true;
+    const uint64_t bit = uint64_t(1) << (dev & 63);
+    if (!(done[wide].load(std::memory_order_acquire) & bit)) {
+      if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return FSB_ERR_CUDA;
+      }
+      done[wide].fetch_or(bit, std::memory_order_release);
+    }
   }
   const int64_t nb = plan.n_block_units;
   const int64_t items = (ceil_div(nb, kRowUnits) + (plan.n_units - nb)) * tiles;
-  int64_t blocks = ceil_div(items, kSpmmWarps);
-  const int64_t resident = resident_blocks(kern, kSpmmWarps * 32, smem);
-  if (blocks > resident) blocks = resident;
+  const int64_t blocks = ceil_div(items, kSpmmWarps);  // one work item per warp, tiles in block order
+  if (items >= (int64_t(1) << 32) || blocks > INT32_MAX || ldb > UINT32_MAX) return FSB_ERR_UNSUPPORTED;
   if (blocks < 1) return FSB_OK;
   kern<<<(unsigned)blocks, kSpmmWarps * 32, smem, st>>>(
-      static_cast<const S*>(data), idx, ptr, static_cast<const S*>(B), ldb, n, static_cast<S*>(C), ldc, plan, T,
-      tiles, spmm_pstride(n), spmm_cps<DT>(n), static_cast<const S*>(x), static_cast<S*>(y));
+      static_cast<const S*>(data), idx, ptr, static_cast<const S*>(B), static_cast<uint32_t>(ldb), n,
+      static_cast<S*>(C), ldc, plan, T, tiles, spmm_pstride(n), spmm_cps<DT>(n), static_cast<const S*>(x),
+      static_cast<S*>(y));
   FSB_LAUNCH_CHECK();
   return FSB_OK;
 }
@@ -1308,8 +1436,8 @@ int spmm_dispatch(const void* data, const int32_t* idx, const int64_t* ptr, cons
   // rows of whole, aligned 16-byte slices: teams of T lanes over column tiles
   // of T * 16 bytes (spmm_team_tile_bytes)
   if (n % kVmax == 0 && ldb % kVmax == 0 && ldc % kVmax == 0 && reinterpret_cast<uintptr_t>(B) % 16 == 0 &&
-      reinterpret_cast<uintptr_t>(C) % 16 == 0) {
-    const int w = spmm_team_tile_bytes(n * int64_t(sizeof(S)), n_cols, plan.tile_bytes);
+      reinterpret_cast<uintptr_t>(C) % 16 == 0 && ldb <= UINT32_MAX && n_cols < (int64_t(1) << 32)) {
+    const int w = spmm_team_tile_bytes(n * int64_t(sizeof(S)), plan.tile_bytes);
     const int T = w / 16;
     return spmm_launch_team<DT, COMP>(data, idx, ptr, B, ldb, n, C, ldc, plan, T, ceil_div(n, int64_t(T) * kVmax),
                                       st);

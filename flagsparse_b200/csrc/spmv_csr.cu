@@ -547,6 +547,64 @@ static int spmv_dispatch_idx(const void* data, const void* idx, int i64, const v
 }
 
 // ---------------------------------------------------------------------------
+// The x-gather floor of a CSR SpMV (measurement only): out[b] = sum of
+// data[i] * x[col[i]] over block b's grid-stride share of all nnz nonzeros,
+// fp64 sums.  It moves the SpMV's values, columns and x gathers with the same
+// load flavours (streaming values / columns, L2-only x) and 8 gathers in
+// flight per thread, without the row structure: its time bounds what any
+// CSR SpMV of the same pattern can reach.
+// ---------------------------------------------------------------------------
+constexpr int kFloorThreads = 256;
+constexpr int kFloorItems = 8;
+
+template <int DT, typename IT>
+__global__ void __launch_bounds__(kFloorThreads)
+k_gather_floor(const typename VT<DT>::Store* __restrict__ data, const IT* __restrict__ col, int64_t nnz,
+               const typename VT<DT>::Store* __restrict__ x, double* __restrict__ out) {
+  using S = typename VT<DT>::Store;
+  __shared__ double red[kFloorThreads / 32];
+  double acc = 0.0;
+  const int64_t step = int64_t(gridDim.x) * kFloorThreads * kFloorItems;
+  for (int64_t base = int64_t(blockIdx.x) * kFloorThreads * kFloorItems; base < nnz; base += step) {
+    S av[kFloorItems], xv[kFloorItems];
+#pragma unroll
+    for (int q = 0; q < kFloorItems; ++q) {
+      const int64_t i = base + q * kFloorThreads + threadIdx.x;
+      if (i < nnz) {
+        av[q] = ld_stream(data + i);
+        xv[q] = ld_x(x + ld_stream(col + i));
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kFloorItems; ++q)
+      if (base + q * kFloorThreads + threadIdx.x < nnz) acc = fma(double(to_real(av[q])), double(to_real(xv[q])), acc);
+  }
+#pragma unroll
+  for (int m = 16; m > 0; m >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, m);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < kFloorThreads / 32; ++w) t += red[w];
+    out[blockIdx.x] = t;
+  }
+}
+
+template <int DT>
+static int gather_floor_launch(const void* data, const void* idx, int i64, int64_t nnz, const void* x, double* out,
+                               int64_t blocks, cudaStream_t st) {
+  using S = typename VT<DT>::Store;
+  if (i64)
+    k_gather_floor<DT, int64_t><<<(unsigned)blocks, kFloorThreads, 0, st>>>(
+        static_cast<const S*>(data), static_cast<const int64_t*>(idx), nnz, static_cast<const S*>(x), out);
+  else
+    k_gather_floor<DT, int32_t><<<(unsigned)blocks, kFloorThreads, 0, st>>>(
+        static_cast<const S*>(data), static_cast<const int32_t*>(idx), nnz, static_cast<const S*>(x), out);
+  FSB_LAUNCH_CHECK();
+  return FSB_OK;
+}
+
+// ---------------------------------------------------------------------------
 // Built-in long-row scratch of fsb_spmv_csr_static_scratch: partial sums of
 // the widest type (c128, 32 bytes) for every slot, then one int32 ticket per
 // slot.  Zero at module load; every call clears the tickets it uses.
@@ -662,6 +720,20 @@ int fsb_spmv_csr(int dtype, const void* data, const void* indices, int idx_is_64
     case FSB_F64: return spmv_dispatch_idx<FSB_F64>(data, indices, idx_is_64, indptr, ptr_is_64, x, y, *plan, st);
     case FSB_C64: return spmv_dispatch_idx<FSB_C64>(data, indices, idx_is_64, indptr, ptr_is_64, x, y, *plan, st);
     case FSB_C128: return spmv_dispatch_idx<FSB_C128>(data, indices, idx_is_64, indptr, ptr_is_64, x, y, *plan, st);
+    default: return FSB_ERR_UNSUPPORTED;
+  }
+}
+
+int fsb_spmv_gather_floor(int dtype, const void* data, const void* indices, int idx_is_64, int64_t nnz,
+                          const void* x, double* out, int64_t n_out, void* stream) {
+  if (nnz < 0 || n_out < 1 || !out || (nnz > 0 && (!data || !indices || !x))) return FSB_ERR_INVALID_ARG;
+  const int64_t blocks = std::min<int64_t>(n_out, int64_t(148) * 8);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  switch (dtype) {
+    case FSB_F16: return gather_floor_launch<FSB_F16>(data, indices, idx_is_64, nnz, x, out, blocks, st);
+    case FSB_BF16: return gather_floor_launch<FSB_BF16>(data, indices, idx_is_64, nnz, x, out, blocks, st);
+    case FSB_F32: return gather_floor_launch<FSB_F32>(data, indices, idx_is_64, nnz, x, out, blocks, st);
+    case FSB_F64: return gather_floor_launch<FSB_F64>(data, indices, idx_is_64, nnz, x, out, blocks, st);
     default: return FSB_ERR_UNSUPPORTED;
   }
 }

@@ -220,6 +220,17 @@ FSB_API int fsb_spmv_csr(int dtype, const void* data, const void* indices, int i
                  const void* x, void* y, const fsb_spmv_plan* plan, void* stream);
 
 /* ------------------------------------------------------------------------
+ * The x-gather floor of a CSR SpMV, for measurement: out[b] (b < the number
+ * of blocks, min(n_out, 1184)) receives the fp64 sum of data[i] * x[indices[i]]
+ * over block b's share of all nnz nonzeros, read with the SpMV's own load
+ * kinds.  Its time is what any SpMV of that pattern needs for its values,
+ * columns and x gathers alone.  Real dtypes (f16, bf16, f32, f64).
+ * No FlagSparse counterpart: a measurement kernel of this library.
+ * ------------------------------------------------------------------------ */
+FSB_API int fsb_spmv_gather_floor(int dtype, const void* data, const void* indices, int idx_is_64, int64_t nnz,
+                          const void* x, double* out, int64_t n_out, void* stream);
+
+/* ------------------------------------------------------------------------
  * CSR SpMV with built-in scratch: allocates nothing on any call.
  *
  * No counterpart in flagos-ai/FlagSparse, whose SpMV allocates its output and

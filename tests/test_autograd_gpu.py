@@ -88,7 +88,7 @@ def test_forward_backward_against_oracle(dname, thresh):
                                           ("float16", 5e-3)])
 def test_gradients_match_torch_sparse_autograd(dname, thresh):
     """Y, dX and dvals against torch's own sparse autograd: torch.sparse.mm on a CPU
-    sparse_csr_tensor whose values are a leaf, float64, on the same rounded inputs
+    sparse_csr_tensor that is a leaf, float64, on the same rounded inputs
     (20,000-node Chung-Lu graph, 64 features).  Half types are compared within
     FlagSparse's thresholds; CPU sparse CSR matmul has no half kernels, so the
     reference runs in float64 as the reference's own tests upcast."""
@@ -102,15 +102,17 @@ def test_gradients_match_torch_sparse_autograd(dname, thresh):
     Y = fs.flagsparse_spmm_csr_autograd(vals, X, prepared=p)
     Y.backward(G)
 
-    v64 = torch.from_numpy(host(vals).astype(np.float64)).requires_grad_(True)
     X64 = torch.from_numpy(host(X).astype(np.float64)).requires_grad_(True)
-    A = torch.sparse_csr_tensor(torch.from_numpy(indptr), torch.from_numpy(indices.astype(np.int64)), v64,
-                                size=shape)
+    crow, colx = torch.from_numpy(indptr), torch.from_numpy(indices.astype(np.int64))
+    A = torch.sparse_csr_tensor(crow, colx, torch.from_numpy(host(vals).astype(np.float64)), size=shape,
+                                requires_grad=True)
     Yt = torch.sparse.mm(A, X64)
     Yt.backward(torch.from_numpy(host(G).astype(np.float64)))
+    # torch's gradient of A lives on A's pattern: its values line up with vals
+    assert torch.equal(A.grad.crow_indices(), crow) and torch.equal(A.grad.col_indices(), colx)
     assert _rel(host(Y).astype(np.float64), Yt.detach().numpy()) <= thresh
     assert _rel(host(X.grad).astype(np.float64), X64.grad.numpy()) <= thresh
-    assert _rel(host(vals.grad).astype(np.float64), v64.grad.numpy()) <= thresh
+    assert _rel(host(vals.grad).astype(np.float64), A.grad.values().numpy()) <= thresh
 
 
 def test_values_change_between_steps():

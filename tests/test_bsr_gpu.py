@@ -118,6 +118,23 @@ def test_bsr16_full_size_sampled_rows_and_determinism():
     assert torch.equal(fs.flagsparse_spmm_bsr16(B=B, prepared=p), C)
 
 
+@pytest.mark.parametrize("N", [128, 192])
+def test_bsr16_b_larger_than_l2(N):
+    """A dense operand larger than L2 (40,000 block columns, K = 640,000 rows), N = 128 and
+    192 (a last tile of 64 columns): every row against the oracle, the error word left clear."""
+    indptr, indices, blocks = _case(300, 40_000, 8, seed=N, empty=(5,))
+    blocks_t = torch.from_numpy(blocks).bfloat16().cuda()
+    g = torch.Generator(device="cuda").manual_seed(N)
+    B = torch.randn(40_000 * 16, N, device="cuda", generator=g).bfloat16()
+    assert B.numel() * 2 > 126 * 2**20
+    p = fs.prepare_spmm_bsr16(blocks_t, torch.from_numpy(indices).cuda(), torch.from_numpy(indptr).cuda(),
+                              (300 * 16, 40_000 * 16))
+    C = fs.flagsparse_spmm_bsr16(B=B, prepared=p)
+    assert p.status(synchronize=True) == 0
+    _check(C, indptr, indices, host(blocks_t), host(B).astype(np.float64), "bfloat16")
+    assert bool((C[5 * 16:6 * 16] == 0).all())
+
+
 def test_bsr16_agrees_with_csr_spmm_on_expanded_matrix():
     indptr, indices, blocks = _case(300, 400, 6, seed=9)
     blocks_t = torch.from_numpy(blocks).bfloat16().cuda()

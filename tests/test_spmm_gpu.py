@@ -123,6 +123,59 @@ def test_spmm_long_rows_multi_chunk(dname, N):
     _check(C, ref, scale, lens, dname, f"zipf {dname} N={N}")
 
 
+def _long_row_matrix(n_long, n_short):
+    """Row 0: n_long nonzeros (value 1) in columns 0 .. n_long-1; row 1: a random row of
+    n_short nonzeros (plain sums); row 2 empty."""
+    rng = np.random.Generator(np.random.PCG64(17))
+    k = n_long + 64
+    cols1 = np.sort(rng.choice(k, n_short, replace=False))
+    indptr = np.array([0, n_long, n_long + n_short, n_long + n_short], dtype=np.int64)
+    indices = np.concatenate([np.arange(n_long), cols1]).astype(np.int32)
+    data = np.concatenate([np.ones(n_long), rng.standard_normal(n_short)])
+    return indptr, indices, data, k
+
+
+def _compensated_bound(dname, ref, scale):
+    """Rows over 1,024 nonzeros: each step's 4 products per team sum plainly, then fold
+    into a compensated (Dot2) accumulator, and the partials combine compensated:
+    |C - exact| <= (u_out + 2 u_acc) |exact| + gamma_6 sum|a||b|, whatever the length."""
+    u, ua = {"bfloat16": 2.0**-8, "float16": 2.0**-11, "float32": 2.0**-24}[dname], 2.0**-24
+    return (u + 2 * ua) * np.abs(ref) + 6 * ua / (1 - 6 * ua) * scale + 1e-30
+
+
+@pytest.mark.parametrize("dname", ["bfloat16", "float16", "float32"])
+@pytest.mark.parametrize("N", [16, 64, 128])
+def test_long_rows_sum_compensated(dname, N):
+    """A 50,000-nonzero row in the fp32-accumulated types sums compensated.  Its first
+    product is +big and its last -big with 49,998 products of `unit` between, unit at or
+    below half an fp32 ulp of big: a plain fp32 sum absorbs every unit term into big and
+    ends at 0, while the compensated sum keeps them (exact: 49,998 unit).  A random row of
+    the same length meets the same bound against the oracle."""
+    dt = TORCH_DT[dname]
+    big, unit = (2.0**15, 2.0**-10) if dname == "float16" else (2.0**24, 1.0)
+    indptr, indices, data, k = _long_row_matrix(50_000, 50)
+    rng = np.random.Generator(np.random.PCG64(N))
+    B = np.full((k, N), unit)
+    B[0] = big
+    B[49_999] = -big
+    B[50_000:] = rng.standard_normal((64, N))
+    C = fs.flagsparse_spmm_csr(dev(data, dt), dev(indices), dev(indptr), dev(B, dt), (3, k))
+    exact = np.full(N, 49_998 * unit)
+    got = host(C[0]).astype(np.float64)
+    assert_within(got, exact, _compensated_bound(dname, exact, np.full(N, 2 * big + 49_998 * unit)),
+                  f"{dname} N={N} cancelling long row")
+    assert np.all(host(C[2]) == 0)
+    d2 = rng.standard_normal(data.size)
+    B2 = rng.standard_normal((k, N))
+    C2 = fs.flagsparse_spmm_csr(dev(d2, dt), dev(indices), dev(indptr), dev(B2, dt), (3, k))
+    d_r, B_r = rounded(d2, dname), rounded(B2, dname)
+    ref = oracle.spmm(indptr, indices, d_r, B_r)
+    scale = oracle.spmm(indptr, indices, np.abs(d_r), np.abs(B_r))
+    got = host(C2).astype(np.float64)
+    assert_within(got[0], ref[0], _compensated_bound(dname, ref[0], scale[0]), f"{dname} N={N} random long row")
+    assert_within(got[1], ref[1], plain_error_bound(dname, ref[1], scale[1], 50), f"{dname} N={N} short row")
+
+
 @pytest.mark.parametrize("route", sorted(sm.SPMM_CSR_ALGORITHMS))
 @pytest.mark.parametrize("dname", ["float32", "float64", "complex64"])
 def test_spmm_every_route(route, dname):
