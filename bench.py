@@ -777,7 +777,7 @@ class BatchedMix:
     rows*4 + cols*16*4 + rows*16*4.
     """
 
-    def __init__(self, device):
+    def __init__(self, device, count=256):
         import torch
 
         import flagsparse_b200 as fs
@@ -785,8 +785,8 @@ class BatchedMix:
 
         self.torch = torch
         self.dtype = "f32"
-        self.name = "batched_256_uneven_f32_spmv_spmm16"
-        mats = workloads.batched_mix()
+        self.name = f"batched_{count}_uneven_f32_spmv_spmm16"
+        mats = workloads.batched_mix(count=count)
         dev = [(torch.from_numpy(m["data"]).to(device), torch.from_numpy(m["indices"]).to(device),
                 torch.from_numpy(m["indptr"]).to(device), m["shape"]) for m in mats]
         b = fs.BatchedCsr(dev, n_dense=16)
@@ -841,7 +841,7 @@ class BatchedMix:
 
 CASES = {
     "gather_floor": lambda d: SpmvGatherFloor(d),
-    "batched_f32": lambda d: BatchedMix(d),
+    "batched_f32": lambda d: BatchedMix(d, BATCH_COUNT),
     "bsr16_bf16_N128": lambda d: Bsr16(d, 128),
     "bsr16_bf16_N64": lambda d: Bsr16(d, 64),
     "bsr_spmv_f32_bd16": lambda d: BsrSpmv(d),
@@ -855,6 +855,9 @@ CASES = {
     "sddmm_bf16_K128": lambda d: AutogradChungLu(d, "bf16", part="sddmm"),
 }
 
+
+# matrices in the batched case (--batched-count; the headline extras use 256)
+BATCH_COUNT = 256
 
 # native kernels per step: the forward SpMM and the one-launch backward
 # (dX and dvals from fsb_spmm_csr_backward).
@@ -901,7 +904,7 @@ def measure_extras(torch, device, flush, peak):
     layer["bf16_speedup_vs_f32"] = round(layer["f32"]["fwd_bwd_ms"] / layer["bf16"]["fwd_bwd_ms"], 3)
     layer["cpu_reference_f32"] = cpu_torch_autograd()
     out["autograd_chung_lu_500k_K128"] = dict(layer, nnz=nnz, error_reference="float64 on the GPU, 500 sampled rows")
-    case = BatchedMix(device)
+    case = BatchedMix(device, 256)
     ms = _event_median_ms(torch, case.step, flush)
     spmv_b, spmm_c, spmm_g = case.b.bytes_models()
     out["batched_256_uneven_f32"] = {"ms": round(ms, 4), "gbs": round((spmv_b + spmm_c) / ms / 1e6, 1),
@@ -1014,7 +1017,11 @@ def main():
     ap.add_argument("--case", default="spmv", choices=["spmv"] + sorted(CASES),
                     help="workload of the timed steps (default: the SpMV headline)")
     ap.add_argument("--mtx", default=None, help="time the SpMV on this MatrixMarket file instead (fp32 values)")
+    ap.add_argument("--batched-count", type=int, default=256,
+                    help="matrices in --case batched_f32 (a smaller batch for profiling)")
     args = ap.parse_args()
+    global BATCH_COUNT
+    BATCH_COUNT = args.batched_count
     args.warmup = max(3, args.warmup)
 
     rank = int(os.environ.get("RANK", "0"))
