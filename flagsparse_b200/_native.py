@@ -62,6 +62,7 @@ class SpmvPlan(ctypes.Structure):
 FSB_SPMV_FAST_SHORT_ROWS = 1
 FSB_SPMV_STATIC_MAX_SLOTS = 65536
 FSB_SPMM_COMPENSATED = 2
+FSB_SPMM_PERSISTENT = 4
 FSB_SDDMM_ACC64 = 1
 FSB_SDDMM_OUT64 = 2
 

@@ -158,6 +158,15 @@ __device__ __forceinline__ int64_t ld_ptr(const P* p, int64_t i) { return static
 }  // namespace fsb
 
 // Status plumbing shared by every C-ABI entry point: never throw, never abort.
+// A grid launched as a programmatic dependent of the grid before it in the
+// stream may start while that grid still runs.  Its last block waits for that
+// grid before exiting, so the dependent grid completes only after both have:
+// work later in the stream sees both grids' results.  Waiting after its own
+// work keeps the overlap.
+__device__ __forceinline__ void pdl_join_primary() {
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 #define FSB_LAUNCH_CHECK()                                   \
   do {                                                       \
     cudaError_t _e = cudaGetLastError();                     \

@@ -322,9 +322,11 @@ __device__ __forceinline__ void stage_offsets(int32_t* sh_off, const int64_t* __
   }
 }
 
-// Rows of more than this many nonzeros accumulate with Dot2 in the types whose
-// sums run in fp32 (f16, bf16, f32), whatever the plan's flags: their sums are
-// the long ones.  Shorter rows keep the plan's accumulation.
+// Rows of more than this many nonzeros accumulate compensated in the types
+// whose sums run in fp32 (f16, bf16, f32), whatever the plan's flags: their
+// sums are the long ones.  Shorter rows keep the plan's accumulation.  The
+// forward kernels use Dot2 (blocked in the team kernel), the backward fp64
+// sums of the exact products.
 constexpr int64_t kCompensateAbove = 1024;
 template <int DT, bool COMP>
 constexpr bool kCompLong = !COMP && (DT == FSB_F16 || DT == FSB_BF16 || DT == FSB_F32);
@@ -1063,6 +1065,52 @@ __device__ __forceinline__ void bwd_put_dots(R (&d)[KA], int base, int stride, i
   }
 }
 
+// fp64 accumulator for a long row of a real type accumulated in fp32 (bf16,
+// f16, f32): each product is exact in fp64 and the fp64 sum of n of them is
+// within n 2^-53 sum|a||b| of the exact sum -- inside the Dot2 bound of the
+// compensated fp32 sum for rows under 2^26 nonzeros, at one DFMA per term and
+// no temporaries.  Partials keep the (hi, lo) fp32 pairs of SpmmAcc<DT, true>.
+template <int DT, int V>
+struct WideAcc {
+  using S = typename VT<DT>::Store;
+  using R = typename VT<DT>::Real;
+  static_assert(std::is_same<R, float>::value, "fp32-accumulated real types only");
+  double s[V];
+
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int j = 0; j < V; ++j) s[j] = 0.0;
+  }
+  __device__ __forceinline__ void add(S a, const S (&b)[V]) {
+    const double ad = to_real(a);
+#pragma unroll
+    for (int j = 0; j < V; ++j) s[j] = fma(ad, double(to_real(b[j])), s[j]);
+  }
+  __device__ __forceinline__ void shfl_add(int m) {
+#pragma unroll
+    for (int j = 0; j < V; ++j) s[j] += __shfl_xor_sync(0xffffffffu, s[j], m);
+  }
+  __device__ __forceinline__ void result(S (&out)[V]) const {
+#pragma unroll
+    for (int j = 0; j < V; ++j) out[j] = spmm_store(__double2float_rn(s[j]), static_cast<S*>(nullptr));
+  }
+  __device__ __forceinline__ void store_partial(R* p) const {
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      const float hi = __double2float_rn(s[j]);
+      p[j * 2] = hi;
+      p[j * 2 + 1] = __double2float_rn(s[j] - double(hi));
+    }
+  }
+  __device__ __forceinline__ void add_partial(const R* p) {
+#pragma unroll
+    for (int j = 0; j < V; ++j) s[j] += double(__ldcg(p + j * 2)) + double(__ldcg(p + j * 2 + 1));
+  }
+};
+
+template <int DT, int V>
+__device__ __forceinline__ void acc_shfl_add(WideAcc<DT, V>& a, int m) { a.shfl_add(m); }
+
 template <int DT, bool DV>
 __global__ void __launch_bounds__(kSpmmWarps * 32, SpmmMinBlocks<DT>::value)
 k_spmm_bwd(const typename VT<DT>::Store* __restrict__ vals, const int32_t* __restrict__ perm,
@@ -1096,31 +1144,14 @@ k_spmm_bwd(const typename VT<DT>::Store* __restrict__ vals, const int32_t* __res
   const int64_t s0 = __ldg(&ud->nnz_begin), s1 = __ldg(&ud->nnz_end);
   const int32_t row = __ldg(&ud->row), tag = __ldg(&ud->tag);
 
-  // stages a batch of <= kSpmmBatch nonzeros: every permutation and column
-  // load issued first, then every value gather, then the stores
+  // stages a batch of <= kSpmmBatch nonzeros (a strided loop: unrolling the
+  // loads ahead costs registers that the gathers below need)
   auto stage = [&](int64_t from, int cnt) {
-    constexpr int kQ = kSpmmBatch / 32;
-    int32_t pv[kQ], cv[kQ];
-    S av[kQ];
-#pragma unroll
-    for (int q = 0; q < kQ; ++q) {
-      const int k = lane + 32 * q;
-      if (k < cnt) {
-        pv[q] = ld_once(perm + from + k);
-        cv[q] = ld_once(col + from + k);
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < kQ; ++q)
-      if (lane + 32 * q < cnt) av[q] = vals[pv[q]];
-#pragma unroll
-    for (int q = 0; q < kQ; ++q) {
-      const int k = lane + 32 * q;
-      if (k < cnt) {
-        sh_p[k] = pv[q];
-        sh_a[k] = av[q];
-        sh_c[k] = cv[q];
-      }
+    for (int k = lane; k < cnt; k += 32) {
+      const int32_t p = ld_once(perm + from + k);
+      sh_p[k] = p;
+      sh_a[k] = vals[p];
+      sh_c[k] = ld_once(col + from + k);
     }
   };
   if (tag >= 0) {
@@ -1180,9 +1211,15 @@ k_spmm_bwd(const typename VT<DT>::Store* __restrict__ vals, const int32_t* __res
 #pragma unroll
     for (int j = 0; j < V; ++j) xf[j] = to_real(xs[j]);
   }
-  // A2: the accumulator of this row's chunks (Dot2 for long rows, see kCompLong)
-  auto run_chunk = [&](auto proto) {
-    using A2 = decltype(proto);
+  // WIDE (rows over kCompensateAbove nonzeros, see kCompLong): fp64 sums of
+  // the exact products (WideAcc) with kA / 2 dY slices in flight, which keeps
+  // the kernel within the plain path's registers (measured on the 500,000-node
+  // Chung-Lu graph, 128 columns: fp32 no slower than plain sums, bf16 3.5 %
+  // slower; Dot2 sums cost 3.5 % / 8 %); else plain sums
+  auto run_chunk = [&](auto wide) {
+    constexpr bool kWide = decltype(wide)::value;
+    using A2 = typename std::conditional<kWide, WideAcc<DT, V>, Acc>::type;
+    constexpr int kAc = kWide ? kA / 2 : kA;
     A2 acc;
     acc.zero();
     for (int64_t b0 = s0; b0 < s1; b0 += kSpmmBatch) {
@@ -1190,22 +1227,22 @@ k_spmm_bwd(const typename VT<DT>::Store* __restrict__ vals, const int32_t* __res
       __syncwarp();
       stage(b0, cnt);
       __syncwarp();
-      for (int k = 0; k < cnt; k += kA * G) {
-        S bv[kA][V];
+      for (int k = 0; k < cnt; k += kAc * G) {
+        S bv[kAc][V];
 #pragma unroll
-        for (int u = 0; u < kA; ++u) {
+        for (int u = 0; u < kAc; ++u) {
           const int kk = k + u * G + team;
           load_slice<S, V>(dY + int64_t(sh_c[kk < cnt ? kk : 0]) * lddy + c0, kk < cnt ? nv : 0, bv[u]);
         }
 #pragma unroll
-        for (int u = 0; u < kA; ++u) {
+        for (int u = 0; u < kAc; ++u) {
           const int kk = k + u * G + team;
           if (kk < cnt) acc.add(sh_a[kk], bv[u]);
         }
         if constexpr (DV) {
-          R d[kA];
-          bwd_dots<S, R, kA, V>(bv, xf, d);
-          bwd_put_dots<S, R, kA>(d, k + team, G, cnt, T, tl, sh_p, dvals);
+          R d[kAc];
+          bwd_dots<S, R, kAc, V>(bv, xf, d);
+          bwd_put_dots<S, R, kAc>(d, k + team, G, cnt, T, tl, sh_p, dvals);
         }
       }
     }
@@ -1240,10 +1277,13 @@ k_spmm_bwd(const typename VT<DT>::Store* __restrict__ vals, const int32_t* __res
     }
     if (lane == 0) plan.counters[first * cps] = 0;  // ready for the next call
   };
-  if (kCompLong<DT, false> && int64_t(nch) * plan.chunk_nnz > kCompensateAbove)
-    run_chunk(SpmmAcc<DT, true, V>());
-  else
-    run_chunk(Acc());
+  if constexpr (kCompLong<DT, false>) {
+    if (int64_t(nch) * plan.chunk_nnz > kCompensateAbove) {
+      run_chunk(std::true_type());
+      return;
+    }
+  }
+  run_chunk(std::false_type());
 }
 
 }  // namespace
@@ -1331,7 +1371,9 @@ int spmm_pick_v(const void* B, int64_t ldb, const void* C, int64_t ldc, int64_t 
 }
 
 // The team kernel: one work item per warp, the items of every tile in tile
-// order (tile bytes = T * 16), so the blocks of one tile run together.
+// order (tile bytes = T * 16), so the blocks of one tile run together; with
+// FSB_SPMM_PERSISTENT, the resident blocks, whose warps stride over the items
+// in the same order.
 template <int DT, bool COMP, bool FUSED = false>
 int spmm_launch_team(const void* data, const int32_t* idx, const int64_t* ptr, const void* B, int64_t ldb, int64_t n,
                      void* C, int64_t ldc, const fsb_spmv_plan& plan, int T, int64_t tiles, cudaStream_t st,
@@ -1358,9 +1400,30 @@ int spmm_launch_team(const void* data, const int32_t* idx, const int64_t* ptr, c
   }
   const int64_t nb = plan.n_block_units;
   const int64_t items = (ceil_div(nb, kRowUnits) + (plan.n_units - nb)) * tiles;
-  const int64_t blocks = ceil_div(items, kSpmmWarps);  // one work item per warp, tiles in block order
+  int64_t blocks = ceil_div(items, kSpmmWarps);  // one work item per warp, tiles in block order
   if (items >= (int64_t(1) << 32) || blocks > INT32_MAX || ldb > UINT32_MAX) return FSB_ERR_UNSUPPORTED;
   if (blocks < 1) return FSB_OK;
+  if (plan.flags & FSB_SPMM_PERSISTENT) {  // the resident blocks; warps stride over the items
+    static std::atomic<int64_t> resident[2][64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+      (void)cudaGetLastError();
+      return FSB_ERR_CUDA;
+    }
+    int64_t r = resident[wide][dev].load(std::memory_order_acquire);
+    if (r == 0) {
+      int per_sm = 0, sms = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kSpmmWarps * 32, smem) != cudaSuccess ||
+          cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || per_sm < 1 ||
+          sms < 1) {
+        (void)cudaGetLastError();
+        return FSB_ERR_CUDA;
+      }
+      r = int64_t(per_sm) * sms;
+      resident[wide][dev].store(r, std::memory_order_release);
+    }
+    if (blocks > r) blocks = r;
+  }
   kern<<<(unsigned)blocks, kSpmmWarps * 32, smem, st>>>(
       static_cast<const S*>(data), idx, ptr, static_cast<const S*>(B), static_cast<uint32_t>(ldb), n,
       static_cast<S*>(C), ldc, plan, T, tiles, spmm_pstride(n), spmm_cps<DT>(n), static_cast<const S*>(x),
@@ -1394,7 +1457,8 @@ int spmm_spmv_fused(const void* data, const int32_t* idx, const int64_t* ptr, co
 
 // dX = A^T dY (and dvals = SDDMM(dY, X) on A's pattern when dvals is given) in
 // one launch of k_spmm_bwd.  Real types, 16-byte aligned rows of at most 512
-// bytes whose width n is a multiple of 16 / sizeof(value), plain sums.
+// bytes whose width n is a multiple of 16 / sizeof(value); plain sums, fp64
+// sums on rows over kCompensateAbove nonzeros for the fp32-accumulated types.
 template <int DT>
 int spmm_backward(const void* vals, const int32_t* perm, const int32_t* idx, const int64_t* ptr, const void* dY,
                   int64_t lddy, const void* X, int64_t ldx, int64_t n, void* dX, int64_t lddx, void* dvals,

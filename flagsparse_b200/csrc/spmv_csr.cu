@@ -257,13 +257,9 @@ struct SpmvLongMinBlocks {
 };
 
 // The long-row launch may start while the row-block launch before it still
-// runs (programmatic dependent launch).  Its last block waits for that grid
-// before exiting, so the long-row grid completes only after both have: work
-// later in the stream sees every y row.  Waiting after its own work keeps
-// the overlap.
-__device__ __forceinline__ void spmv_long_join() {
-  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) asm volatile("griddepcontrol.wait;" ::: "memory");
-}
+// runs (programmatic dependent launch); pdl_join_primary makes its grid
+// complete only after both have, so work later in the stream sees every y row.
+__device__ __forceinline__ void spmv_long_join() { pdl_join_primary(); }
 
 // LONG = true: the long-row chunks units[unit0, unit1), no shared memory (the
 // gathers of long rows run faster with the L1 capacity that row-block staging

@@ -256,10 +256,11 @@ class SpmmPlan:
     def n_slots(self):
         return self.plan.n_slots
 
-    def struct_for(self, n, compensated=False, tile_bytes=0):
+    def struct_for(self, n, compensated=False, tile_bytes=0, persistent=False):
         """ctypes reference to an fsb_spmv_plan with scratch for dense width ``n``.
 
-        ``tile_bytes``: column tile of the team kernel (0 = the library's choice)."""
+        ``tile_bytes``: column tile of the team kernel (0 = the library's choice);
+        ``persistent``: the team kernel's persistent grid (FSB_SPMM_PERSISTENT)."""
         key = int(n)
         entry = self._scratch.get(key)
         if entry is None:
@@ -276,7 +277,7 @@ class SpmmPlan:
             entry = (partials, counters, st)
             self._scratch[key] = entry
         st = entry[2]
-        st.flags = nat.FSB_SPMM_COMPENSATED if compensated else 0
+        st.flags = (nat.FSB_SPMM_COMPENSATED if compensated else 0) | (nat.FSB_SPMM_PERSISTENT if persistent else 0)
         st.tile_bytes = int(tile_bytes)
         return ctypes.byref(st)
 
@@ -285,7 +286,7 @@ class SpmmPlan:
         return all(int(c.abs().sum().item()) == 0 for _, c, _ in self._scratch.values())
 
 
-def spmm_spmv(data, indices, indptr, n_rows, n_cols, B, plan, out, x, y, compensated=False):
+def spmm_spmv(data, indices, indptr, n_rows, n_cols, B, plan, out, x, y, compensated=False, persistent=False):
     """out = A @ B and y = A @ x in one launch through fsb_spmm_spmv_csr.
 
     Returns False (nothing launched) when the fused kernel does not apply
@@ -296,7 +297,7 @@ def spmm_spmv(data, indices, indptr, n_rows, n_cols, B, plan, out, x, y, compens
         nat.dtype_code(data.dtype), nat.ptr(data), nat.ptr(indices), nat.ptr(indptr), int(n_rows), int(n_cols),
         nat.ptr(B), int(B.stride(0)) if B.shape[0] > 1 else max(n, 1), n, nat.ptr(out),
         int(out.stride(0)) if out.shape[0] > 1 else max(n, 1), nat.ptr(x), nat.ptr(y),
-        plan.struct_for(n, compensated), nat.stream_of(out.device),
+        plan.struct_for(n, compensated, persistent=persistent), nat.stream_of(out.device),
     )
     if rc == nat.FSB_ERR_UNSUPPORTED:
         return False
@@ -329,19 +330,21 @@ def spmm_backward(vals, perm32, t_indices, t_indptr, n_rows, n_cols, dY, X, dX, 
     return True
 
 
-def spmm(data, indices, indptr, n_rows, n_cols, B, plan, out, compensated=False, tile_bytes=0):
+def spmm(data, indices, indptr, n_rows, n_cols, B, plan, out, compensated=False, tile_bytes=0, persistent=False):
     """out[:n_rows, :N] = A @ B through fsb_spmm_csr.
 
     ``indices`` int32, ``indptr`` int64, ``B`` and ``out`` row-major 2-D with
     unit column stride; ``plan`` a SpmmPlan of this matrix; ``tile_bytes`` the
-    column tile of the team kernel (0 = the library's choice).
+    column tile of the team kernel (0 = the library's choice); ``persistent``
+    its persistent grid.
     """
     n = int(B.shape[1])
     nat.check(
         nat.lib().fsb_spmm_csr(
             nat.dtype_code(data.dtype), nat.ptr(data), nat.ptr(indices), nat.ptr(indptr), int(n_rows), int(n_cols),
             nat.ptr(B), int(B.stride(0)) if B.shape[0] > 1 else max(n, 1), n, nat.ptr(out),
-            int(out.stride(0)) if out.shape[0] > 1 else max(n, 1), plan.struct_for(n, compensated, tile_bytes),
+            int(out.stride(0)) if out.shape[0] > 1 else max(n, 1),
+            plan.struct_for(n, compensated, tile_bytes, persistent),
             nat.stream_of(out.device),
         ),
         "fsb_spmm_csr",

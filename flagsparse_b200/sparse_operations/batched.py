@@ -18,7 +18,8 @@ with one view per matrix; ``capture()`` records the step in a CUDA graph and
 
 ``tune()`` is the schedule autotuner: it times candidate plan parameters (the
 row-block window ``cap`` and the long-row chunk of the SpMV and the SpMM
-plans) and the fused step on this batch and keeps the fastest schedule;
+plans, and for the best SpMM shape the persistent grid against one work item
+per warp) and the fused step on this batch and keeps the fastest schedule;
 results are cached per batch signature (dtype, width, row-length histogram)
 in memory and, when a path is given, in a JSON file.
 """
@@ -133,12 +134,17 @@ class BatchedCsr:
             "fsb_spmv_csr",
         )
 
-    def _launch_spmm(self, plan):
-        _csr.spmm(self.data, self.indices, self.indptr, self.n_rows, self.n_cols, self.B, plan, self.C)
+    def _launch_spmm(self, plan, persistent=None):
+        if persistent is None:
+            persistent = bool(self.spmm_cfg.get("persistent", False))
+        _csr.spmm(self.data, self.indices, self.indptr, self.n_rows, self.n_cols, self.B, plan, self.C,
+                  persistent=persistent)
 
-    def _launch_fused(self, plan):
+    def _launch_fused(self, plan, persistent=None):
+        if persistent is None:
+            persistent = bool(self.spmm_cfg.get("persistent", False))
         return _csr.spmm_spmv(self.data, self.indices, self.indptr, self.n_rows, self.n_cols, self.B, plan, self.C,
-                              self.x, self.y)
+                              self.x, self.y, persistent=persistent)
 
     def step(self):
         """y = A x and C = A B over the whole batch (no graph): the fused launch when
@@ -187,18 +193,32 @@ class BatchedCsr:
             report["spmv_trials"].append(dict(cfg, ms=round(ms, 5)))
             if best_v is None or ms < best_v[1]:
                 best_v = (cfg, ms)
-        fusable = self._launch_fused(self._spmm_plan_get())
+        fusable = self._launch_fused(self._spmm_plan_get(), persistent=False)
+        # each plan shape with one work item per warp, then the best one also on the
+        # persistent grid (same results, another schedule of the same items)
         for cfg in SPMM_CANDIDATES:
+            cfg = dict(cfg, persistent=False)
             plan = _csr.SpmmPlan(self.indptr, self.n_rows, self.dtype, cap=cfg["cap"], chunk_nnz=cfg["chunk"])
-            ms = self._time(lambda: self._launch_spmm(plan))
+            ms = self._time(lambda: self._launch_spmm(plan, False))
             report["spmm_trials"].append(dict(cfg, ms=round(ms, 5)))
             if best_m is None or ms < best_m[1]:
                 best_m = (cfg, ms)
             if fusable:
-                ms = self._time(lambda: self._launch_fused(plan))
+                ms = self._time(lambda: self._launch_fused(plan, False))
                 report["fused_trials"].append(dict(cfg, ms=round(ms, 5)))
                 if best_f is None or ms < best_f[1]:
                     best_f = (cfg, ms)
+        def persistent_trial(best, launch, trials):
+            if best is None:
+                return best
+            cfg = dict(best[0], persistent=True)
+            plan = _csr.SpmmPlan(self.indptr, self.n_rows, self.dtype, cap=cfg["cap"], chunk_nnz=cfg["chunk"])
+            ms = self._time(lambda: launch(plan, True))
+            report[trials].append(dict(cfg, ms=round(ms, 5)))
+            return (cfg, ms) if ms < best[1] else best
+
+        best_m = persistent_trial(best_m, self._launch_spmm, "spmm_trials")
+        best_f = persistent_trial(best_f, self._launch_fused, "fused_trials")
         self.fused = best_f is not None and best_f[1] < best_v[1] + best_m[1]
         self.spmv_cfg = dict(best_v[0])
         self.spmm_cfg = dict(best_f[0] if self.fused else best_m[0])

@@ -294,6 +294,11 @@ FSB_API int fsb_spmv_csr_static_scratch(int dtype, const void* data, const void*
  * (spmm_csr.py:2452-2544) launch.
  * ------------------------------------------------------------------------ */
 #define FSB_SPMM_COMPENSATED 2
+/* Team kernel (rows of whole 16-byte slices): a persistent grid of the
+ * resident blocks whose warps stride over the work items, instead of one work
+ * item per warp.  Results are identical either way; the batched step's
+ * autotuner times both. */
+#define FSB_SPMM_PERSISTENT 4
 
 FSB_API int32_t fsb_spmm_default_cap(int dtype);
 FSB_API int32_t fsb_spmm_default_chunk(int dtype);
@@ -329,8 +334,9 @@ FSB_API int fsb_spmm_spmv_csr(int dtype, const void* data, const int32_t* indice
  * FSB_ERR_UNSUPPORTED otherwise, with nothing launched; the caller then runs
  * fsb_gather_values + fsb_spmm_csr and fsb_sddmm_csr.  t_plan: A^T's SpMM plan
  * with scratch for this n (as for fsb_spmm_csr).  dX sums in fp32 (fp64 for
- * f64) in a fixed order; each dvals entry sums in fp32 (fp64) over a fixed
- * tree.  No FlagSparse counterpart: it has no autograd for CSR SpMM. */
+ * f64) in a fixed order, A^T rows of more than 1,024 nonzeros in fp64 from
+ * exact products (f16, bf16, f32); each dvals entry sums in fp32 (fp64) over
+ * a fixed tree.  No FlagSparse counterpart: it has no autograd for CSR SpMM. */
 FSB_API int fsb_spmm_csr_backward(int dtype, const void* vals, const int32_t* perm, const int32_t* t_indices,
                           const int64_t* t_indptr, int64_t n_rows, int64_t n_cols, const void* dY, int64_t lddy,
                           const void* X, int64_t ldx, int64_t n, void* dX, int64_t lddx, void* dvals,

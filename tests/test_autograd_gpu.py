@@ -8,7 +8,7 @@ import torch
 import flagsparse_b200 as fs
 from flagsparse_b200 import workloads
 from oracle import oracle
-from tests.helpers import dev, host, op_csr
+from tests.helpers import dev, host, op_csr, spmv_error_bound
 
 pytestmark = pytest.mark.gpu
 
@@ -151,3 +151,43 @@ def test_autograd_full_size_bf16_sampled():
     got = host(X.grad[torch.from_numpy(rows).cuda()]).astype(np.float64)
     assert _rel(got, dX_ref) <= 1e-2
     assert torch.isfinite(vals.grad.float()).all()
+
+
+@pytest.mark.parametrize("dname", ["bfloat16", "float32"])
+@pytest.mark.parametrize("N", [16, 128])
+def test_backward_long_column_sums_compensated(dname, N):
+    """dX = A^T dY sums A's columns: column 0 holds 50,000 ones, and dY's rows 0 and
+    49,999 are +big and -big with `unit` rows between (unit at or below half an fp32 ulp of
+    big).  A plain fp32 sum absorbs every unit term and ends at 0; the backward sums rows
+    over 1,024 nonzeros in fp64 (exact products), so dX[0] = 49,998 unit within the bound
+    of a compensated (Dot2) sum, which the fp64 sum meets with room to spare.  dvals and
+    the other columns stay within FlagSparse's thresholds of the fp64 oracle."""
+    dt = getattr(torch, dname)
+    n_long, k = 50_000, 8
+    rng = np.random.Generator(np.random.PCG64(N))
+    # row r < n_long: (r, 0) and one entry in columns 1..k-1; rows beyond: short random rows
+    rows = [np.array([0, 1 + r % (k - 1)]) for r in range(n_long)] + [np.sort(rng.choice(k, 3, replace=False))
+                                                                       for _ in range(32)]
+    indptr = np.zeros(len(rows) + 1, dtype=np.int64)
+    np.cumsum([len(r) for r in rows], out=indptr[1:])
+    indices = np.concatenate(rows).astype(np.int32)
+    data = np.ones(indices.size)
+    shape = (len(rows), k)
+    big, unit = 2.0**24, 1.0
+    G = np.full((shape[0], N), unit)
+    G[0], G[n_long - 1] = big, -big
+    G[n_long:] = rng.standard_normal((32, N))
+    X = rng.standard_normal((k, N))
+    vals = dev(data, dt).requires_grad_(True)
+    Xd = dev(X, dt).requires_grad_(True)
+    p = fs.prepare_spmm_csr_autograd(vals.detach(), dev(indices), dev(indptr), shape)
+    fs.flagsparse_spmm_csr_autograd(vals, Xd, prepared=p).backward(dev(G, dt))
+    exact = np.full(N, (n_long - 2) * unit)
+    S = np.full(N, 2 * big + (n_long - 2) * unit)
+    got = host(Xd.grad[0]).astype(np.float64)
+    bound = spmv_error_bound(dname, exact, S, n_long)
+    assert np.all(np.abs(got - exact) <= bound), (got[:4], bound[:4])
+    _, dXo, dvo = _oracle_grads(indptr, indices, data, host(Xd).astype(np.float64), host(dev(G, dt)).astype(np.float64),
+                                shape)
+    assert _rel(host(Xd.grad).astype(np.float64)[1:], dXo[1:]) <= (1e-2 if dname == "bfloat16" else 1e-6)
+    assert _rel(host(vals.grad).astype(np.float64), dvo) <= (1e-2 if dname == "bfloat16" else 1e-6)

@@ -67,16 +67,19 @@ def test_batched_autotuner_picks_and_caches(tmp_path):
     bm._TUNE_CACHE.clear()
     rep = b.tune(cache_path=path)
     assert rep["source"] == "measured"
-    assert len(rep["spmv_trials"]) == len(bm.SPMV_CANDIDATES) and len(rep["spmm_trials"]) == len(bm.SPMM_CANDIDATES)
+    # every SpMM shape on one work item per warp, plus the best one on the persistent grid
+    assert len(rep["spmv_trials"]) == len(bm.SPMV_CANDIDATES)
+    assert len(rep["spmm_trials"]) == len(bm.SPMM_CANDIDATES) + 1
+    assert [t["persistent"] for t in rep["spmm_trials"]].count(True) == 1
     # fp32 with a 16-column B: the one-kernel step applies and is timed too
-    assert len(rep["fused_trials"]) == len(bm.SPMM_CANDIDATES)
+    assert len(rep["fused_trials"]) == len(bm.SPMM_CANDIDATES) + 1
     fastest_v = min(rep["spmv_trials"], key=lambda t: t["ms"])
     fastest_m = min(rep["spmm_trials"], key=lambda t: t["ms"])
     fastest_f = min(rep["fused_trials"], key=lambda t: t["ms"])
     assert rep["fused"] == (fastest_f["ms"] < fastest_v["ms"] + fastest_m["ms"]) == b.fused
     best = fastest_f if b.fused else fastest_m
     assert b.spmv_cfg == {"cap": fastest_v["cap"], "chunk": fastest_v["chunk"]}
-    assert b.spmm_cfg == {"cap": best["cap"], "chunk": best["chunk"]}
+    assert b.spmm_cfg == {"cap": best["cap"], "chunk": best["chunk"], "persistent": best["persistent"]}
     b.run()
     torch.cuda.synchronize()
     _check_all(b, mats, "tuned")
