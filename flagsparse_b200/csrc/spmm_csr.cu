@@ -595,12 +595,63 @@ __device__ __forceinline__ void acc_fold(SpmmAcc<DT, true, V>& a, const SpmmAcc<
     for (int j = 0; j < V; ++j) a.s[c][j].add(t.s[c][j].hi);
 }
 
+// fp64 accumulator for a long row of a real type accumulated in fp32 (bf16,
+// f16, f32): each product is exact in fp64 and the fp64 sum of n of them is
+// within n 2^-53 sum|a||b| of the exact sum -- inside the Dot2 bound of the
+// compensated fp32 sum for rows under 2^26 nonzeros, at one DFMA per term and
+// no temporaries.  Partials keep the (hi, lo) fp32 pairs of SpmmAcc<DT, true>.
+template <int DT, int V>
+struct WideAcc {
+  using S = typename VT<DT>::Store;
+  using R = typename VT<DT>::Real;
+  static_assert(std::is_same<R, float>::value, "fp32-accumulated real types only");
+  static constexpr int kNC = 1;  // real components per element
+  double s[V];
+
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int j = 0; j < V; ++j) s[j] = 0.0;
+  }
+  __device__ __forceinline__ void add(S a, const S (&b)[V]) {
+    const double ad = to_real(a);
+#pragma unroll
+    for (int j = 0; j < V; ++j) s[j] = fma(ad, double(to_real(b[j])), s[j]);
+  }
+  __device__ __forceinline__ void shfl_add(int m) {
+#pragma unroll
+    for (int j = 0; j < V; ++j) s[j] += __shfl_xor_sync(0xffffffffu, s[j], m);
+  }
+  __device__ __forceinline__ void result(S (&out)[V]) const {
+#pragma unroll
+    for (int j = 0; j < V; ++j) out[j] = spmm_store(__double2float_rn(s[j]), static_cast<S*>(nullptr));
+  }
+  __device__ __forceinline__ void store_partial(R* p) const {
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+      const float hi = __double2float_rn(s[j]);
+      p[j * 2] = hi;
+      p[j * 2 + 1] = __double2float_rn(s[j] - double(hi));
+    }
+  }
+  __device__ __forceinline__ void add_partial(const R* p) {
+#pragma unroll
+    for (int j = 0; j < V; ++j) s[j] += double(__ldcg(p + j * 2)) + double(__ldcg(p + j * 2 + 1));
+  }
+};
+
+template <int DT, int V>
+__device__ __forceinline__ void acc_shfl_add(WideAcc<DT, V>& a, int m) { a.shfl_add(m); }
+
 // Accumulation of a long-row chunk: MODE 0 plain sums; 1 Dot2 on every term
 // (plans with FSB_SPMM_COMPENSATED); 2 blocked compensation: each step's
-// kSpmmAhead products of a team are summed plainly, then folded into a Dot2
-// accumulator, so the error is at most gamma_(kSpmmAhead+1) * sum|a||b| plus
+// KA products of a team are summed plainly, then folded into a Dot2
+// accumulator, so the error is at most gamma_(KA+1) * sum|a||b| plus
 // the final rounding whatever the row length (the chunk and team partials
-// are combined compensated as well).
+// are combined compensated as well); 3 fp64 sums of the exact products
+// (WideAcc), far inside that bound.  Modes 2 and 3 serve the same rows of
+// the fp32-accumulated types: 3 in the one-team kernel, where it measured
+// faster (fp32, 128 columns: 2.21 against 2.25 ms), 2 elsewhere (fp64 sums
+// cost 4-5 % on 256-byte rows).
 template <int DT, int MODE, int V>
 struct ChunkAcc;
 template <int DT, int V>
@@ -609,12 +660,14 @@ template <int DT, int V>
 struct ChunkAcc<DT, 1, V> { using T = SpmmAcc<DT, true, V>; };
 template <int DT, int V>
 struct ChunkAcc<DT, 2, V> { using T = SpmmAcc<DT, true, V>; };
+template <int DT, int V>
+struct ChunkAcc<DT, 3, V> { using T = WideAcc<DT, V>; };
 
-// One long-row chunk of the team kernel: team g takes nonzeros g, g+G, ...;
-// the team partials are combined by xor-shuffles over the team index, then
-// the chunk is stored directly (one-chunk rows) or as a slot partial whose
-// ticket's last taker adds the partials in chunk order.
-template <int DT, int MODE, bool FUSED>
+// One long-row chunk of the team kernel: team g takes nonzeros g, g+G, ...,
+// KA B-row slices in flight; the team partials are combined by xor-shuffles
+// over the team index, then the chunk is stored directly (one-chunk rows) or
+// as a slot partial whose ticket's last taker adds the partials in chunk order.
+template <int DT, int MODE, bool FUSED, int KA>
 __device__ __forceinline__ void team_chunk(const typename VT<DT>::Store* __restrict__ data,
                                            const int32_t* __restrict__ col,
                                            const typename VT<DT>::Store* __restrict__ B, uint32_t ldb, int64_t n,
@@ -644,43 +697,43 @@ __device__ __forceinline__ void team_chunk(const typename VT<DT>::Store* __restr
     __syncwarp();
     const S* sv = sh_a + stage_nz<S, kRowStage>(sh_a, sh_c, data, col, b0, cnt, lane);
     __syncwarp();
-    for (int k = 0; k < cnt; k += kSpmmAhead * G) {
-      S bv[kSpmmAhead][V];
-      S xv[kSpmmAhead];
+    for (int k = 0; k < cnt; k += KA * G) {
+      S bv[KA][V];
+      S xv[KA];
 #pragma unroll
-      for (int q = 0; q < kSpmmAhead; ++q) {
+      for (int q = 0; q < KA; ++q) {
         const int kk = k + q * G + team;
         load_row16<S, V>(Bl, static_cast<uint32_t>(sh_c[kk < cnt ? kk : cnt - 1]), ldb, bv[q]);
       }
       if constexpr (FUSED) {
-        // the y terms of these kSpmmAhead * G items, one per lane in order
+        // the y terms of these KA * G items, one per lane in order
 #pragma unroll
-        for (int q = 0; q * 32 < kSpmmAhead * G; ++q) {
+        for (int q = 0; q * 32 < KA * G; ++q) {
           const int kk = k + q * 32 + lane;
-          if (q * 32 + lane < kSpmmAhead * G && kk < cnt) xv[q] = ld_gather(x + sh_c[kk]);
+          if (q * 32 + lane < KA * G && kk < cnt) xv[q] = ld_gather(x + sh_c[kk]);
         }
       }
       if constexpr (MODE == 2) {
         SpmmAcc<DT, false, V> step;
         step.zero();
 #pragma unroll
-        for (int q = 0; q < kSpmmAhead; ++q) {
+        for (int q = 0; q < KA; ++q) {
           const int kk = k + q * G + team;
           if (kk < cnt) step.add(sv[kk], bv[q]);
         }
         acc_fold(acc, step);
       } else {
 #pragma unroll
-        for (int q = 0; q < kSpmmAhead; ++q) {
+        for (int q = 0; q < KA; ++q) {
           const int kk = k + q * G + team;
           if (kk < cnt) acc.add(sv[kk], bv[q]);
         }
       }
       if constexpr (FUSED) {
 #pragma unroll
-        for (int q = 0; q * 32 < kSpmmAhead * G; ++q) {
+        for (int q = 0; q * 32 < KA * G; ++q) {
           const int kk = k + q * 32 + lane;
-          if (q * 32 + lane < kSpmmAhead * G && kk < cnt) yacc.add_prod(to_real(sv[kk]), to_real(xv[q]));
+          if (q * 32 + lane < KA * G && kk < cnt) yacc.add_prod(to_real(sv[kk]), to_real(xv[q]));
         }
       }
     }
@@ -951,17 +1004,23 @@ k_spmm_team(const typename VT<DT>::Store* __restrict__ data, const int32_t* __re
     // ------------------------------------------------------------ long-row chunk
     const fsb_spmv_unit* ud = plan.units + nb + (item - n_groups);
     const int32_t nch = __ldg(&ud->n_chunks);
-    // rows of more than kCompensateAbove nonzeros sum with Dot2 (compensated)
-    // accumulators in the fp32-accumulated types, partials and all
-    if constexpr (COMP)
-      team_chunk<DT, 1, FUSED>(data, col, B, ldb, n, C, ldc, plan, ud, T, tile, c0, nv, pstride, cps, x, y, sh_a,
-                               sh_c);
-    else if (kCompLong<DT, COMP> && int64_t(nch) * plan.chunk_nnz > kCompensateAbove)
-      team_chunk<DT, 2, FUSED>(data, col, B, ldb, n, C, ldc, plan, ud, T, tile, c0, nv, pstride, cps, x, y, sh_a,
-                               sh_c);
-    else
-      team_chunk<DT, 0, FUSED>(data, col, B, ldb, n, C, ldc, plan, ud, T, tile, c0, nv, pstride, cps, x, y, sh_a,
-                               sh_c);
+    // rows of more than kCompensateAbove nonzeros sum compensated in the
+    // fp32-accumulated types, partials and all (blocked Dot2, or fp64 sums
+    // in the one-team kernel)
+    if constexpr (COMP) {
+      team_chunk<DT, 1, FUSED, KP>(data, col, B, ldb, n, C, ldc, plan, ud, T, tile, c0, nv, pstride, cps, x, y,
+                                   sh_a, sh_c);
+      continue;
+    }
+    if constexpr (kCompLong<DT, COMP>) {
+      if (int64_t(nch) * plan.chunk_nnz > kCompensateAbove) {
+        team_chunk<DT, (KP > kSpmmAhead ? 3 : 2), FUSED, KP>(data, col, B, ldb, n, C, ldc, plan, ud, T, tile, c0, nv,
+                                                             pstride, cps, x, y, sh_a, sh_c);
+        continue;
+      }
+    }
+    team_chunk<DT, 0, FUSED, KP>(data, col, B, ldb, n, C, ldc, plan, ud, T, tile, c0, nv, pstride, cps, x, y, sh_a,
+                                 sh_c);
   }
 }
 
@@ -1064,52 +1123,6 @@ __device__ __forceinline__ void bwd_put_dots(R (&d)[KA], int base, int stride, i
     if (i < held && k < limit) dvals[sh_p[k]] = spmm_store(d[i], static_cast<S*>(nullptr));
   }
 }
-
-// fp64 accumulator for a long row of a real type accumulated in fp32 (bf16,
-// f16, f32): each product is exact in fp64 and the fp64 sum of n of them is
-// within n 2^-53 sum|a||b| of the exact sum -- inside the Dot2 bound of the
-// compensated fp32 sum for rows under 2^26 nonzeros, at one DFMA per term and
-// no temporaries.  Partials keep the (hi, lo) fp32 pairs of SpmmAcc<DT, true>.
-template <int DT, int V>
-struct WideAcc {
-  using S = typename VT<DT>::Store;
-  using R = typename VT<DT>::Real;
-  static_assert(std::is_same<R, float>::value, "fp32-accumulated real types only");
-  double s[V];
-
-  __device__ __forceinline__ void zero() {
-#pragma unroll
-    for (int j = 0; j < V; ++j) s[j] = 0.0;
-  }
-  __device__ __forceinline__ void add(S a, const S (&b)[V]) {
-    const double ad = to_real(a);
-#pragma unroll
-    for (int j = 0; j < V; ++j) s[j] = fma(ad, double(to_real(b[j])), s[j]);
-  }
-  __device__ __forceinline__ void shfl_add(int m) {
-#pragma unroll
-    for (int j = 0; j < V; ++j) s[j] += __shfl_xor_sync(0xffffffffu, s[j], m);
-  }
-  __device__ __forceinline__ void result(S (&out)[V]) const {
-#pragma unroll
-    for (int j = 0; j < V; ++j) out[j] = spmm_store(__double2float_rn(s[j]), static_cast<S*>(nullptr));
-  }
-  __device__ __forceinline__ void store_partial(R* p) const {
-#pragma unroll
-    for (int j = 0; j < V; ++j) {
-      const float hi = __double2float_rn(s[j]);
-      p[j * 2] = hi;
-      p[j * 2 + 1] = __double2float_rn(s[j] - double(hi));
-    }
-  }
-  __device__ __forceinline__ void add_partial(const R* p) {
-#pragma unroll
-    for (int j = 0; j < V; ++j) s[j] += double(__ldcg(p + j * 2)) + double(__ldcg(p + j * 2 + 1));
-  }
-};
-
-template <int DT, int V>
-__device__ __forceinline__ void acc_shfl_add(WideAcc<DT, V>& a, int m) { a.shfl_add(m); }
 
 template <int DT, bool DV>
 __global__ void __launch_bounds__(kSpmmWarps * 32, SpmmMinBlocks<DT>::value)

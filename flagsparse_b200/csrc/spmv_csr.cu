@@ -114,6 +114,29 @@ struct SpmvAcc<DT, COMP, false> {
   }
 };
 
+// Short rows of the fp32 SpMV: fp64 sums of the exact products (an fp32
+// product is exact in fp64, and the fp64 sum of a row-block row is far inside
+// the Dot2 bound), staged as the two words of the double in the hi / lo
+// slots.  One DADD per term instead of Dot2's six additions: the row-block
+// launch is issue-bound, and the SpMV of the 2M x 2M Zipf(2) matrix took
+// 0.200 against 0.204 ms.
+struct SpmvWideF32 {
+  static constexpr bool kLo = true;
+  double c;
+  __device__ __forceinline__ void zero() { c = 0.0; }
+  __device__ __forceinline__ static void prod(float a, float x, float* hi, float* lo) {
+    const double p = __dmul_rn(double(a), double(x));
+    hi[0] = __int_as_float(__double2loint(p));
+    lo[0] = __int_as_float(__double2hiint(p));
+  }
+  __device__ __forceinline__ void add_rec(const float* hi, const float* lo) {
+    c = __dadd_rn(c, __hiloint2double(__float_as_int(lo[0]), __float_as_int(hi[0])));
+  }
+  __device__ __forceinline__ void combine(const SpmvWideF32& o) { c = __dadd_rn(c, o.c); }
+  __device__ __forceinline__ void shfl_up(int o) { c = __shfl_up_sync(0xffffffffu, c, o); }
+  __device__ __forceinline__ float result() const { return __double2float_rn(c); }
+};
+
 template <int DT, bool COMP>
 struct SpmvAcc<DT, COMP, true> {
   using Tr = SpmvTraits<DT>;
@@ -364,7 +387,7 @@ k_spmv_csr(const typename VT<DT>::Store* __restrict__ data, const IT* __restrict
   for (int64_t uid = unit; uid < unit1; uid += stride) {
   UnitRegs nxt = u;
   if (uid + stride < unit1) nxt = load_unit(plan.units + uid + stride);
-  using SAcc = SpmvAcc<DT, SHORT_COMP>;
+  using SAcc = typename std::conditional<DT == FSB_F32 && SHORT_COMP, SpmvWideF32, SpmvAcc<DT, SHORT_COMP>>::type;
   constexpr bool kLo = SAcc::kLo;
   const int64_t r0 = u.row;
   const int nr = u.tag - u.row;
