@@ -569,6 +569,44 @@ class SpmmPowerLaw:
         return _max_rel(self.C[torch.from_numpy(rows).to(self.C.device)].double(), ref)
 
 
+class SpmmGatherTma(SpmmPowerLaw):
+    """The B-row gather floor of the same SpMM through TMA (fsb_spmm_gather_floor_tma):
+    every nonzero's B row copied by tile::gather4 into per-warp shared-memory rings and
+    summed, with no row structure (3 CTAs of 4 warps per SM).  value is reported on the
+    SpMM's byte model, so it reads as the SpMM's GB/s if its B rows moved that way."""
+
+    def __init__(self, device, dname="f32", n=128):
+        super().__init__(device, dname, n)
+        from flagsparse_b200 import _native as nat
+
+        self.nat = nat
+        self.name = f"spmm_gather_tma_powerlaw_1Mx1M_{dname}_N{n}"
+        self.out = self.torch.zeros(148 * 3 * 4, n, dtype=self.torch.float32, device=device)
+        self.err = self.torch.zeros(1, dtype=self.torch.int32, device=device)
+
+    def step(self):
+        nat = self.nat
+        nat.check(nat.lib().fsb_spmm_gather_floor_tma(nat.dtype_code(self.vals.dtype), nat.ptr(self.vals),
+                                                      nat.ptr(self.ind), self.nnz, nat.ptr(self.B), self.K,
+                                                      int(self.B.stride(0)), self.n, nat.ptr(self.out),
+                                                      self.out.shape[0], nat.ptr(self.err),
+                                                      nat.stream_of(self.B.device)),
+                  "fsb_spmm_gather_floor_tma")
+
+    def e2e_step(self):
+        self.B_dev2.copy_(self.B_host, non_blocking=True)
+        self.step()
+
+    def e2e_bytes(self):
+        return self.K * self.n * self.s, 0
+
+    def launches_per_step(self):
+        return 1
+
+    def max_rel_err(self, rows, take, owner):
+        return None
+
+
 class AutogradChungLu:
     """Y = A X forward and dX = A^T dY, dvals = SDDMM(dY, X) backward on the 500,000-node
     Chung-Lu graph (mean degree 25, seed 3), 128 features.
@@ -849,6 +887,8 @@ CASES = {
     "spmm_f32_N64": lambda d: SpmmPowerLaw(d, "f32", 64),
     "spmm_f32_N128": lambda d: SpmmPowerLaw(d, "f32", 128),
     "spmm_bf16_N128": lambda d: SpmmPowerLaw(d, "bf16", 128),
+    "spmm_gather_tma_f32_N128": lambda d: SpmmGatherTma(d, "f32", 128),
+    "spmm_gather_tma_bf16_N128": lambda d: SpmmGatherTma(d, "bf16", 128),
     "autograd_f32": lambda d: AutogradChungLu(d, "f32"),
     "autograd_bf16": lambda d: AutogradChungLu(d, "bf16"),
     "sddmm_f32_K128": lambda d: AutogradChungLu(d, "f32", part="sddmm"),

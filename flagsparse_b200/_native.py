@@ -143,6 +143,9 @@ _SIGNATURES = {
     "fsb_spmv_gather_floor": (
         _c_int, [_c_int, _c_ptr, _c_ptr, _c_int, _c_i64, _c_ptr, _c_ptr, _c_i64, _c_ptr],
     ),
+    "fsb_spmm_gather_floor_tma": (
+        _c_int, [_c_int, _c_ptr, _c_ptr, _c_i64, _c_ptr, _c_i64, _c_i64, _c_i64, _c_ptr, _c_i64, _c_ptr, _c_ptr],
+    ),
     "fsb_spmv_csr_static_scratch": (
         _c_int,
         [_c_int, _c_ptr, _c_ptr, _c_int, _c_ptr, _c_int, _c_i64, _c_i64, _c_ptr, _c_ptr,

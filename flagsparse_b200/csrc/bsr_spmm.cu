@@ -38,6 +38,7 @@
 #include <cudaTypedefs.h>
 
 #include "fsb_common.cuh"
+#include "fsb_tma.cuh"
 
 namespace fsb {
 namespace {
@@ -52,7 +53,6 @@ constexpr int kBsrTileM = 128;                        // dense columns per MMA
 constexpr int kSlabBytes = 16 * kBsrTileM * 2;        // B slab: 16 rows x 128 columns, 2-byte values
 constexpr int kBlkBytes = 16 * 16 * 2;                // one 16 x 16 block
 constexpr int kTmemCols = 32;                         // two 16-column fp32 accumulators
-constexpr uint32_t kWaitLimit = 1u << 24;             // bounded mbarrier polls
 
 // Shared-memory operand layouts:
 //   slab (MMA A, MN-major, SWIZZLE_128B): two 64-column halves 2048 bytes apart
@@ -62,10 +62,6 @@ constexpr uint32_t kWaitLimit = 1u << 24;             // bounded mbarrier polls
 //     (n/8)*256 + (k/8)*128 + (n%8)*16 + (k%8)*2 -> SBO 256, LBO 128
 constexpr uint32_t kSlabLBO = 2048, kSlabSBO = 1024, kBlkSBO = 256, kBlkLBO = 128;
 constexpr uint32_t kLayoutNone = 0, kLayoutSw128 = 2;
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
 
 // UMMA shared-memory descriptor: start address, leading / stride byte offsets
 // (all >> 4), version 1, base offset 0 (swizzle atoms are 1024-byte aligned),
@@ -85,49 +81,6 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
 __host__ __device__ constexpr uint32_t umma_idesc(uint32_t ab_format) {
   return (1u << 4) | (ab_format << 7) | (ab_format << 10) | (1u << 15) | (0u << 16) | ((16u >> 3) << 17) |
          ((uint32_t(kBsrTileM) >> 4) << 24);
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
-}
-
-// Returns false if the phase with the given parity did not complete within the
-// poll limit, or (when abort is given) once another role has set *abort.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const volatile int* abort = nullptr) {
-  for (uint32_t i = 0; i < kWaitLimit; ++i) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    if (done) return true;
-    if (abort && (i & 255u) == 255u && *abort) return false;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-
-// 2-D TMA tile load (no multicast) completing on an mbarrier
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int32_t x, int32_t y, uint32_t bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
-          "r"(dst),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
-      : "memory");
-}
-
-// contiguous bulk copy global -> shared (16-byte aligned, size a multiple of 16)
-__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-               "l"(src), "r"(bytes), "r"(bar)
-               : "memory");
 }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -347,21 +300,6 @@ __global__ void k_bsr16_pack(const uint4* __restrict__ src, uint4* __restrict__ 
     const int a = static_cast<int>(i & 31), n = a >> 1, k8 = a & 1;
     dst[b * 32 + ((n >> 3) * 256 + k8 * 128 + (n & 7) * 16) / 16] = src[i];
   }
-}
-
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    else
-      (void)cudaGetLastError();
-  });
-  return fn;
 }
 
 template <typename S>

@@ -231,6 +231,25 @@ FSB_API int fsb_spmv_gather_floor(int dtype, const void* data, const void* indic
                           const void* x, double* out, int64_t n_out, void* stream);
 
 /* ------------------------------------------------------------------------
+ * The B-row gather floor of the CSR SpMM through TMA (measurement kernel).
+ *
+ * out[w * n + j] = sum over nonzeros i in [w * per, min(nnz, (w + 1) * per))
+ * of data[i] * B[indices[i] * ldb + j], fp32 sums, for w < out_rows and
+ * j < n, per = ceil(nnz / out_rows): every nonzero's B row and no row
+ * structure.  Rows of B are copied four at a time by cp.async.bulk.tensor
+ * tile::gather4 into per-warp shared-memory rings (one CTA per 4 warps,
+ * out_rows / 4 CTAs).  dtype f32, bf16 or f16 with n * sizeof(value) = 256
+ * or 512 bytes (else FSB_ERR_UNSUPPORTED); indices int32 in [0, k_rows);
+ * B 16-byte aligned with ldb * sizeof(value) a
+ * multiple of 16; out_rows a positive multiple of 4.  *err (device int) is
+ * set to 1 if a copy did not land within the wait limit, leaving out
+ * partial.  No FlagSparse counterpart: a measurement kernel of this library.
+ * ------------------------------------------------------------------------ */
+FSB_API int fsb_spmm_gather_floor_tma(int dtype, const void* data, const int32_t* indices, int64_t nnz,
+                                      const void* B, int64_t k_rows, int64_t ldb, int64_t n, float* out,
+                                      int64_t out_rows, int* err, void* stream);
+
+/* ------------------------------------------------------------------------
  * CSR SpMV with built-in scratch: allocates nothing on any call.
  *
  * No counterpart in flagos-ai/FlagSparse, whose SpMV allocates its output and
