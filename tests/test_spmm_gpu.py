@@ -293,10 +293,12 @@ def test_spmm_repeat_calls_bitwise_and_tickets_reset():
     assert plan.n_slots > 0 and plan.counters_clear()
 
 
-@pytest.mark.parametrize("dname,N", [("float32", 16), ("float32", 128), ("bfloat16", 64), ("float64", 32)])
-def test_spmm_persistent_grid_bitwise(dname, N):
+@pytest.mark.parametrize("dname,N,tile", [("float32", 16, 0), ("float32", 128, 0), ("bfloat16", 64, 0),
+                                         ("float64", 32, 0), ("float32", 128, 128), ("bfloat16", 256, 256)])
+def test_spmm_persistent_grid_bitwise(dname, N, tile):
     """The persistent grid (FSB_SPMM_PERSISTENT) runs the same work items as one item per
-    warp, so the products are bitwise equal -- also for the fused SpMV + SpMM launch."""
+    warp, so the products are bitwise equal -- with narrower column tiles too, and for the
+    fused SpMV + SpMM launch."""
     c = workloads.zipf_csr(n=300_000, seed=21, dtype=np.float64)
     dt = TORCH_DT[dname]
     data, ind, ptr = dev(c["data"], dt), dev(c["indices"]), dev(c["indptr"])
@@ -305,7 +307,7 @@ def test_spmm_persistent_grid_bitwise(dname, N):
     B = torch.randn(c["shape"][1], N, device="cuda", dtype=torch.float64).to(dt)
     C = [torch.empty(n, N, device="cuda", dtype=dt) for _ in range(2)]
     for C_i, persistent in zip(C, (False, True)):
-        _csr.spmm(data, ind, ptr, n, c["shape"][1], B, plan, C_i, persistent=persistent)
+        _csr.spmm(data, ind, ptr, n, c["shape"][1], B, plan, C_i, tile_bytes=tile, persistent=persistent)
     assert torch.equal(C[0], C[1])
     ref, scale, lens = _oracle_spmm(c["indptr"], c["indices"], rounded(c["data"], dname), c["shape"],
                                     rounded(host(B), dname), "non")
