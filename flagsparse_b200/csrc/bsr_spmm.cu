@@ -46,8 +46,12 @@ namespace {
 constexpr int kBsrThreads = 192;                      // warps 0-3 epilogue, 4 producer, 5 MMA
 // 7 CTAs per SM with a 4-deep ring each: more independent block pipelines per
 // SM measured faster than fewer, deeper ones (N = 64: 0.23 ms against 0.32 ms
-// with 4 CTAs x 8 stages; N = 128: 0.362 against 0.366 ms).
+// with 4 CTAs x 8 stages; N = 128: 0.362 against 0.366 ms).  Products of at
+// most 64 columns (one half-filled tile, half-size slab copies) run 8 per SM:
+// 0.222 against 0.242 ms on 65,536^2 blocks, where N = 128 measured 0.369
+// against 0.366 ms (6 stages at 7 per SM: 0.248 / 0.384 ms).
 constexpr int kBsrCtasPerSm = 7;
+constexpr int kBsrCtasPerSmNarrow = 8;
 constexpr int kBsrStages = 4;
 constexpr int kBsrTileM = 128;                        // dense columns per MMA
 constexpr int kSlabBytes = 16 * kBsrTileM * 2;        // B slab: 16 rows x 128 columns, 2-byte values
@@ -135,7 +139,7 @@ __device__ __forceinline__ void bsr_fail(int* err, volatile int* abort) {
 
 // grid: x = CTAs over contiguous block-row ranges, y = 128-column tiles of C.
 template <typename S>
-__global__ void __launch_bounds__(kBsrThreads, kBsrCtasPerSm)
+__global__ void __launch_bounds__(kBsrThreads, kBsrCtasPerSmNarrow)
 k_bsr16_spmm(const __grid_constant__ CUtensorMap tmap_b, const S* __restrict__ packed, const int32_t* __restrict__ bcol,
              const int64_t* __restrict__ bptr, int64_t n_brows, int64_t rows_per_cta, S* __restrict__ C, int64_t ldc,
              int64_t n, uint32_t idesc, int tile_cols, int* __restrict__ err) {
@@ -323,7 +327,7 @@ int bsr_launch(CUtensorMapDataType tdt, uint32_t ab_format, const void* packed, 
   const int tile_cols = kBsrTileM;
   const int64_t tiles = ceil_div(n, tile_cols);
   if (tiles > 65535) return FSB_ERR_UNSUPPORTED;
-  const int64_t target = 148 * kBsrCtasPerSm;  // resident CTAs
+  const int64_t target = 148 * (n <= 64 ? kBsrCtasPerSmNarrow : kBsrCtasPerSm);  // resident CTAs
   const int64_t rows_per_cta = ceil_div(n_brows, target);
   const int64_t grid_x = ceil_div(n_brows, rows_per_cta);
   dim3 grid((unsigned)grid_x, (unsigned)tiles);
