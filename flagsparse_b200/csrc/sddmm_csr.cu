@@ -189,6 +189,25 @@ template <> struct Widen<double> {
   }
 };
 
+// acc += lo(x) * lo(y), then acc += hi(x) * hi(y) for two packed 16-bit
+// values each: sm_100a's mixed-precision fma.rn.f32.{bf16,f16} multiplies the
+// 16-bit inputs exactly (their product fits fp32) and rounds the sum once,
+// so the result equals widening both to fp32 and calling fmaf, in the same
+// order, with no widening instructions.
+template <typename S>
+__device__ __forceinline__ float fma_pair16(unsigned xw, unsigned yw, float acc) {
+  if constexpr (std::is_same<S, __nv_bfloat16>::value) {
+    asm("{\n .reg .b16 xl, xh, yl, yh;\n mov.b32 {xl, xh}, %1;\n mov.b32 {yl, yh}, %2;\n"
+        " fma.rn.f32.bf16 %0, xl, yl, %0;\n fma.rn.f32.bf16 %0, xh, yh, %0;\n}"
+        : "+f"(acc) : "r"(xw), "r"(yw));
+  } else {
+    asm("{\n .reg .b16 xl, xh, yl, yh;\n mov.b32 {xl, xh}, %1;\n mov.b32 {yl, yh}, %2;\n"
+        " fma.rn.f32.f16 %0, xl, yl, %0;\n fma.rn.f32.f16 %0, xh, yh, %0;\n}"
+        : "+f"(acc) : "r"(xw), "r"(yw));
+  }
+  return acc;
+}
+
 // 16-byte slice at p, or only its first nv elements (the rest zero).
 template <typename S>
 __device__ __forceinline__ uint4 slice16(const S* p, int nv) {
@@ -236,12 +255,17 @@ k_sddmm_team(const int32_t* __restrict__ row_ids, const int32_t* __restrict__ co
     nvt[t] = static_cast<int>(k - off[t] >= VW ? int64_t(VW) : (k > off[t] ? k - off[t] : int64_t(0)));
   }
   const R a = static_cast<R>(alpha), b = static_cast<R>(beta);
+  // 16-bit values: x rows stay packed and multiply through fma_pair16
+  constexpr bool kMixed = sizeof(S) == 2;
   int cur = -1;
   R xf[TILES][VW];
+  uint4 xw[TILES];
 #pragma unroll
-  for (int t = 0; t < TILES; ++t)
+  for (int t = 0; t < TILES; ++t) {
+    xw[t] = make_uint4(0u, 0u, 0u, 0u);
 #pragma unroll
     for (int j = 0; j < VW; ++j) xf[t][j] = R(0);
+  }
 
   for (int r0 = 0; r0 < cnt; r0 += PER_ROUND) {
     const int first = r0 + team * kTeamU;  // this team's items: first .. first+3
@@ -267,14 +291,24 @@ k_sddmm_team(const int32_t* __restrict__ row_ids, const int32_t* __restrict__ co
         if (rq[u] != cur) {  // uniform inside the team
           cur = rq[u];
 #pragma unroll
-          for (int t = 0; t < TILES; ++t) W::run(slice16<S>(x + int64_t(cur) * ldx + off[t], nvt[t]), xf[t]);
+          for (int t = 0; t < TILES; ++t) {
+            if constexpr (kMixed) xw[t] = slice16<S>(x + int64_t(cur) * ldx + off[t], nvt[t]);
+            else W::run(slice16<S>(x + int64_t(cur) * ldx + off[t], nvt[t]), xf[t]);
+          }
         }
 #pragma unroll
         for (int t = 0; t < TILES; ++t) {
-          R yf[VW];
-          W::run(yw[u][t], yf);
+          if constexpr (kMixed) {
+            part[u] = fma_pair16<S>(xw[t].x, yw[u][t].x, part[u]);
+            part[u] = fma_pair16<S>(xw[t].y, yw[u][t].y, part[u]);
+            part[u] = fma_pair16<S>(xw[t].z, yw[u][t].z, part[u]);
+            part[u] = fma_pair16<S>(xw[t].w, yw[u][t].w, part[u]);
+          } else {
+            R yf[VW];
+            W::run(yw[u][t], yf);
 #pragma unroll
-          for (int j = 0; j < VW; ++j) part[u] = fma(xf[t][j], yf[j], part[u]);
+            for (int j = 0; j < VW; ++j) part[u] = fma(xf[t][j], yf[j], part[u]);
+          }
         }
       }
     }

@@ -121,6 +121,26 @@ __device__ __forceinline__ void ffma2(float& c0, float& c1, float a, float b0, f
   asm("mov.b64 {%0, %1}, %2;" : "=f"(c0), "=f"(c1) : "l"(cc));
 }
 
+// (c0, c1) += (a * lo(b), a * hi(b)) for a 16-bit a and two packed 16-bit
+// values b: sm_100a's mixed-precision fma.rn.f32.{bf16,f16} multiplies the
+// 16-bit inputs exactly (the product fits fp32) and rounds each sum once, so
+// the results equal widening to fp32 and calling fmaf, with no widening
+// instructions.
+template <typename S>
+__device__ __forceinline__ void fma_mixed2(float& c0, float& c1, S a, unsigned b) {
+  unsigned short ab;
+  memcpy(&ab, &a, 2);
+  if constexpr (std::is_same<S, __nv_bfloat16>::value) {
+    asm("{\n .reg .b16 bl, bh;\n mov.b32 {bl, bh}, %3;\n fma.rn.f32.bf16 %0, %2, bl, %0;\n"
+        " fma.rn.f32.bf16 %1, %2, bh, %1;\n}"
+        : "+f"(c0), "+f"(c1) : "h"(ab), "r"(b));
+  } else {
+    asm("{\n .reg .b16 bl, bh;\n mov.b32 {bl, bh}, %3;\n fma.rn.f32.f16 %0, %2, bl, %0;\n"
+        " fma.rn.f32.f16 %1, %2, bh, %1;\n}"
+        : "+f"(c0), "+f"(c1) : "h"(ab), "r"(b));
+  }
+}
+
 // Per-lane accumulator of V output elements.
 template <int DT, bool COMP, int V>
 struct SpmmAcc {
@@ -155,7 +175,12 @@ struct SpmmAcc {
       }
     } else {
       const R ar = to_real(a);
-      if constexpr (!COMP && std::is_same<R, float>::value && V % 2 == 0) {
+      if constexpr (!COMP && sizeof(S) == 2 && V % 2 == 0) {
+        unsigned bw[V / 2];
+        memcpy(bw, b, sizeof(bw));
+#pragma unroll
+        for (int j = 0; j < V; j += 2) fma_mixed2(s[0][j].hi, s[0][j + 1].hi, a, bw[j / 2]);
+      } else if constexpr (!COMP && std::is_same<R, float>::value && V % 2 == 0) {
 #pragma unroll
         for (int j = 0; j < V; j += 2) ffma2(s[0][j].hi, s[0][j + 1].hi, ar, to_real(b[j]), to_real(b[j + 1]));
       } else {
@@ -1090,11 +1115,35 @@ __device__ __forceinline__ void ffma2x(float& c0, float& c1, float a0, float a1,
 
 // Per-lane partial dot products of the kA dY slices with this lane's X slice
 // (already widened to R); fp32 sums run as two packed halves added at the end.
+// (c0, c1) += (lo(x) * lo(b), hi(x) * hi(b)) for packed 16-bit x and b, one
+// rounding each (see fma_mixed2).
+template <typename S>
+__device__ __forceinline__ void fma_mixed2x(float& c0, float& c1, unsigned x, unsigned b) {
+  if constexpr (std::is_same<S, __nv_bfloat16>::value) {
+    asm("{\n .reg .b16 xl, xh, bl, bh;\n mov.b32 {xl, xh}, %2;\n mov.b32 {bl, bh}, %3;\n"
+        " fma.rn.f32.bf16 %0, bl, xl, %0;\n fma.rn.f32.bf16 %1, bh, xh, %1;\n}"
+        : "+f"(c0), "+f"(c1) : "r"(x), "r"(b));
+  } else {
+    asm("{\n .reg .b16 xl, xh, bl, bh;\n mov.b32 {xl, xh}, %2;\n mov.b32 {bl, bh}, %3;\n"
+        " fma.rn.f32.f16 %0, bl, xl, %0;\n fma.rn.f32.f16 %1, bh, xh, %1;\n}"
+        : "+f"(c0), "+f"(c1) : "r"(x), "r"(b));
+  }
+}
+
+// xs: the same X slice as xf, unwidened (16-bit values multiply from it).
 template <typename S, typename R, int KA, int V>
-__device__ __forceinline__ void bwd_dots(const S (&bv)[KA][V], const R (&xf)[V], R (&d)[KA]) {
+__device__ __forceinline__ void bwd_dots(const S (&bv)[KA][V], const R (&xf)[V], const S (&xs)[V], R (&d)[KA]) {
 #pragma unroll
   for (int u = 0; u < KA; ++u) {
-    if constexpr (std::is_same<R, float>::value && V % 2 == 0) {
+    if constexpr (sizeof(S) == 2 && V % 2 == 0) {
+      unsigned xw[V / 2], bw[V / 2];
+      memcpy(xw, xs, sizeof(xw));
+      memcpy(bw, bv[u], sizeof(bw));
+      float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+      for (int j = 0; j < V / 2; ++j) fma_mixed2x<S>(s0, s1, xw[j], bw[j]);
+      d[u] = s0 + s1;
+    } else if constexpr (std::is_same<R, float>::value && V % 2 == 0) {
       float s0 = 0.f, s1 = 0.f;
 #pragma unroll
       for (int j = 0; j < V; j += 2) ffma2x(s0, s1, to_real(bv[u][j]), to_real(bv[u][j + 1]), xf[j], xf[j + 1]);
@@ -1182,8 +1231,8 @@ k_spmm_bwd(const typename VT<DT>::Store* __restrict__ vals, const int32_t* __res
       int maxlen = len;
       for (int m = T; m < 32; m <<= 1) maxlen = max(maxlen, __shfl_xor_sync(0xffffffffu, maxlen, m));
       R xf[V];
+      S xs[V];
       if constexpr (DV) {
-        S xs[V];
         load_slice<S, V, true>(X + (int64_t(row) + (has ? i : 0)) * ldx + c0, len > 0 ? nv : 0, xs);
 #pragma unroll
         for (int j = 0; j < V; ++j) xf[j] = to_real(xs[j]);
@@ -1202,7 +1251,7 @@ k_spmm_bwd(const typename VT<DT>::Store* __restrict__ vals, const int32_t* __res
           if (k + u < len) acc.add(sh_a[b + k + u], bv[u]);
         if constexpr (DV) {
           R d[kA];
-          bwd_dots<S, R, kA, V>(bv, xf, d);
+          bwd_dots<S, R, kA, V>(bv, xf, xs, d);
           bwd_put_dots<S, R, kA>(d, b + k, 1, b + len, T, tl, sh_p, dvals);
         }
       }
@@ -1218,8 +1267,8 @@ k_spmm_bwd(const typename VT<DT>::Store* __restrict__ vals, const int32_t* __res
   // ------------------------------------------------------------ long-row chunk
   const int32_t nch = __ldg(&ud->n_chunks), slot = __ldg(&ud->slot);
   R xf[V];
+  S xs[V];
   if constexpr (DV) {
-    S xs[V];
     load_slice<S, V, true>(X + int64_t(row) * ldx + c0, nv, xs);
 #pragma unroll
     for (int j = 0; j < V; ++j) xf[j] = to_real(xs[j]);
@@ -1254,7 +1303,7 @@ k_spmm_bwd(const typename VT<DT>::Store* __restrict__ vals, const int32_t* __res
         }
         if constexpr (DV) {
           R d[kAc];
-          bwd_dots<S, R, kAc, V>(bv, xf, d);
+          bwd_dots<S, R, kAc, V>(bv, xf, xs, d);
           bwd_put_dots<S, R, kAc>(d, k + team, G, cnt, T, tl, sh_p, dvals);
         }
       }
